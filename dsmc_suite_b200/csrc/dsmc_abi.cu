@@ -1,0 +1,608 @@
+// dsmc_abi.cu - implementation of the C ABI in include/dsmc_cuda.h: contexts, uploads,
+// launches and result copies. Everything here is host code; the kernels live in kernel_*.cu.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "dsmc_cuda.h"
+#include "dsmc_kernels.h"
+#include "fast_engine.h"
+
+extern "C" {
+#include "types.h"
+#include "velocity.h"
+}
+
+using dsmc::DevTables;
+
+struct dsmc_ctx {
+    int device = -1;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    bool ready = false;
+    dsmc_params params{};
+    DevTables t{};
+    long long ncell = 0, nhcell = 0, nhist = 0;
+    std::vector<void *> tables;     // owned device allocations of the current problem
+    void *outputs[3] = {nullptr, nullptr, nullptr};  // ttime, fate, steps
+    unsigned long long *stats = nullptr;
+    dsmc::FastEngine *fast = nullptr;
+    char err[512] = {0};
+};
+
+namespace {
+
+thread_local char g_create_err[512];
+
+int fail(dsmc_ctx *c, int status, const char *fmt, ...) {
+    char *buf = c ? c->err : g_create_err;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, 512, fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+#define DSMC_CUDA_TRY(ctx, call)                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail((ctx), e_ == cudaErrorMemoryAllocation ? DSMC_ERR_NO_MEMORY     \
+                                                               : DSMC_ERR_CUDA,         \
+                        "%s: %s", #call, cudaGetErrorString(e_));                       \
+    } while (0)
+
+int set_device(dsmc_ctx *c) {
+    DSMC_CUDA_TRY(c, cudaSetDevice(c->device));
+    return DSMC_OK;
+}
+
+void free_tables(dsmc_ctx *c) {
+    for (void *p : c->tables) cudaFree(p);
+    c->tables.clear();
+    c->ready = false;
+}
+
+void free_outputs(dsmc_ctx *c) {
+    for (void *&p : c->outputs) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    c->t.ttime = nullptr;
+    c->t.fate = nullptr;
+    c->t.steps = nullptr;
+    c->t.out_cap = 0;
+    c->t.out_base = 0;
+}
+
+// Allocate and upload one host array (nullptr host -> nullptr device).
+template <typename T, typename D>
+int upload(dsmc_ctx *c, const T *host, size_t count, D **dev) {
+    static_assert(sizeof(T) == sizeof(D), "element size mismatch");
+    *dev = nullptr;
+    if (!host || count == 0) return DSMC_OK;
+    void *p = nullptr;
+    DSMC_CUDA_TRY(c, cudaMalloc(&p, count * sizeof(T)));
+    c->tables.push_back(p);
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    *dev = static_cast<D *>(p);
+    return DSMC_OK;
+}
+
+template <typename T>
+int alloc_zero(dsmc_ctx *c, size_t count, T **dev) {
+    void *p = nullptr;
+    DSMC_CUDA_TRY(c, cudaMalloc(&p, count * sizeof(T)));
+    c->tables.push_back(p);
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(p, 0, count * sizeof(T), c->stream));
+    *dev = static_cast<T *>(p);
+    return DSMC_OK;
+}
+
+int check_params(dsmc_ctx *c, const dsmc_params *p, const dsmc_surface *s,
+                 const dsmc_collision *col) {
+    if (!p || !s) return fail(c, DSMC_ERR_INVALID, "params and surface are required");
+    if (p->ftd < 1 || p->ffd < 1 || p->hd < 1 || p->ftd > 4096 || p->ffd > 4096 || p->hd > 4096)
+        return fail(c, DSMC_ERR_INVALID, "grid dimensions out of range");
+    if (!(p->dt_step > 0.0) || !(p->Radii > 0.0) || !(p->GM > 0.0) || !(p->max_height > p->Radii))
+        return fail(c, DSMC_ERR_INVALID, "dt, Radii, GM and max_height must be positive");
+    if (p->hop_step_cap < 1) return fail(c, DSMC_ERR_INVALID, "hop_step_cap must be >= 1");
+    if (p->model == DSMC_MODEL_REFERENCE) {
+        if (!s->T_map) return fail(c, DSMC_ERR_INVALID, "reference model needs T_map");
+    } else if (p->model == DSMC_MODEL_CONFIG) {
+        if (!s->face_verts || !s->face_T || !s->base_centroid || !s->split_planes ||
+            s->nlevel < 0 || s->nlevel > 6 || s->nface != (20 << (2 * s->nlevel)))
+            return fail(c, DSMC_ERR_INVALID, "config model needs a complete icosphere surface");
+    } else {
+        return fail(c, DSMC_ERR_INVALID, "unknown model %d", p->model);
+    }
+    if (p->runner != DSMC_RUNNER_BALLISTIC && p->runner != DSMC_RUNNER_ADVANCED)
+        return fail(c, DSMC_ERR_INVALID, "unknown runner %d", p->runner);
+    if (col && col->n_bg) {
+        if (!col->cdf_coef || !col->cdf_box || !col->cdf_total || !col->cdf_valid ||
+            col->cdf_degree < 0 || col->cdf_degree > DSMC_CDF_MAX_DEGREE || col->n_bg_len < 0)
+            return fail(c, DSMC_ERR_INVALID, "incomplete collision tables");
+    }
+    if (p->n_speed_bins < 0 || p->n_speed_bins > 1024 ||
+        (p->n_speed_bins > 0 && !(p->speed_bin_width > 0.0)))
+        return fail(c, DSMC_ERR_INVALID, "bad speed histogram shape");
+    return DSMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dsmc_status_string(int status) {
+    switch (status) {
+        case DSMC_OK: return "ok";
+        case DSMC_ERR_INVALID: return "invalid argument";
+        case DSMC_ERR_CUDA: return "CUDA error";
+        case DSMC_ERR_NO_DEVICE: return "no CUDA device";
+        case DSMC_ERR_NO_MEMORY: return "out of memory";
+        case DSMC_ERR_STATE: return "call out of order";
+        case DSMC_ERR_BUDGET: return "memory budget exceeded";
+        case DSMC_ERR_IO: return "file I/O error";
+        default: return "unknown status";
+    }
+}
+
+const char *dsmc_last_error(const dsmc_ctx *ctx) { return ctx ? ctx->err : g_create_err; }
+
+int dsmc_ctx_create(int device, dsmc_ctx **out) {
+    if (!out) return fail(nullptr, DSMC_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(nullptr, DSMC_ERR_NO_DEVICE, "no CUDA device (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= n)
+        return fail(nullptr, DSMC_ERR_NO_DEVICE, "device %d out of range (%d devices)", device, n);
+    dsmc_ctx *c = new (std::nothrow) dsmc_ctx();
+    if (!c) return fail(nullptr, DSMC_ERR_NO_MEMORY, "host allocation failed");
+    c->device = device;
+    int rc = set_device(c);
+    if (rc == DSMC_OK) {
+        e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaMalloc(&c->stats, dsmc::kStatCount * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemset(c->stats, 0, dsmc::kStatCount * sizeof(unsigned long long));
+        if (e != cudaSuccess) rc = fail(nullptr, DSMC_ERR_CUDA, "context set-up: %s", cudaGetErrorString(e));
+    } else {
+        snprintf(g_create_err, sizeof g_create_err, "%s", c->err);
+    }
+    if (rc != DSMC_OK) {
+        if (c->stats) cudaFree(c->stats);
+        if (c->own_stream) cudaStreamDestroy(c->own_stream);
+        delete c;
+        return rc;
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return DSMC_OK;
+}
+
+int dsmc_ctx_destroy(dsmc_ctx *c) {
+    if (!c) return DSMC_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    delete c->fast;
+    free_tables(c);
+    free_outputs(c);
+    if (c->stats) cudaFree(c->stats);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return DSMC_OK;
+}
+
+int dsmc_ctx_set_stream(dsmc_ctx *c, void *stream) {
+    if (!c) return DSMC_ERR_INVALID;
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    return DSMC_OK;
+}
+
+int dsmc_setup(dsmc_ctx *c, const dsmc_params *p, const dsmc_surface *s,
+               const dsmc_collision *col) {
+    if (!c) return DSMC_ERR_INVALID;
+    int rc = check_params(c, p, s, col);
+    if (rc != DSMC_OK) return rc;
+    if ((rc = set_device(c)) != DSMC_OK) return rc;
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    free_tables(c);
+    DevTables &t = c->t;
+    const double *out_ttime = t.ttime;
+    int *out_fate = t.fate;
+    long long *out_steps = t.steps;
+    long long out_cap = t.out_cap;
+    t = DevTables{};
+    t.ttime = const_cast<double *>(out_ttime);
+    t.fate = out_fate;
+    t.steps = out_steps;
+    t.out_cap = out_cap;
+    c->params = *p;
+    const long long ftd = p->ftd, ffd = p->ffd, hd = p->hd;
+    c->ncell = hd * ftd * ffd;
+    c->nhcell = ftd * ffd;
+    c->nhist = p->n_speed_bins > 0 ? c->ncell * p->n_speed_bins : 0;
+
+    if (p->model == DSMC_MODEL_REFERENCE) {
+        // Launch-speed table, built on the host with the reference's constants
+        // (include/constants.h:17-23 and src/common/velocity.c:6-47).
+        static VelocityTable vt;
+        velocity_table_init(&vt, 18e-3, 6.02e23, 1.38e-23);
+        const double *d_T = nullptr;
+        if ((rc = upload(c, s->T_map, static_cast<size_t>(ftd * ffd), &d_T)) != DSMC_OK) return rc;
+        t.T_map = d_T;
+        double *d_sp = nullptr;
+        int *d_cnt = nullptr;
+        if ((rc = upload(c, &vt.speeds[0][0], 23 * 1000, &d_sp)) != DSMC_OK) return rc;
+        if ((rc = upload(c, vt.count, 23, &d_cnt)) != DSMC_OK) return rc;
+        // The upload is asynchronous: keep the static table stable until the copy is done.
+        DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        t.vt_speeds = d_sp;
+        t.vt_count = d_cnt;
+    } else {
+        const size_t nf = static_cast<size_t>(s->nface);
+        const size_t nnode = static_cast<size_t>(20 * ((1 << (2 * s->nlevel)) - 1) / 3);
+        t.nface = s->nface;
+        t.nlevel = s->nlevel;
+        const double *dv = nullptr, *dT = nullptr, *dc = nullptr, *db = nullptr, *dp = nullptr;
+        if ((rc = upload(c, s->face_verts, nf * 9, &dv)) != DSMC_OK) return rc;
+        if ((rc = upload(c, s->face_T, nf, &dT)) != DSMC_OK) return rc;
+        if ((rc = upload(c, s->face_cdf, nf, &dc)) != DSMC_OK) return rc;
+        if ((rc = upload(c, s->base_centroid, static_cast<size_t>(60), &db)) != DSMC_OK) return rc;
+        if ((rc = upload(c, s->split_planes, nnode * 9, &dp)) != DSMC_OK) return rc;
+        t.face_verts = dv; t.face_T = dT; t.face_cdf = dc; t.base_centroid = db; t.split_planes = dp;
+    }
+    if (col && col->n_bg) {
+        const size_t nc = static_cast<size_t>(c->ncell);
+        const double *nb = nullptr, *cc = nullptr, *cb = nullptr, *ct = nullptr;
+        const int *cv = nullptr;
+        if ((rc = upload(c, col->n_bg, static_cast<size_t>(col->n_bg_len), &nb)) != DSMC_OK) return rc;
+        if ((rc = upload(c, col->cdf_coef, nc * DSMC_CDF_STRIDE, &cc)) != DSMC_OK) return rc;
+        if ((rc = upload(c, col->cdf_box, nc * 4, &cb)) != DSMC_OK) return rc;
+        if ((rc = upload(c, col->cdf_total, nc, &ct)) != DSMC_OK) return rc;
+        if ((rc = upload(c, reinterpret_cast<const int *>(col->cdf_valid), nc, &cv)) != DSMC_OK) return rc;
+        t.n_bg = nb; t.n_bg_len = col->n_bg_len; t.cdf_coef = cc; t.cdf_box = cb; t.cdf_total = ct;
+        t.cdf_valid = cv; t.cdf_degree = col->cdf_degree;
+    }
+    if ((rc = alloc_zero(c, static_cast<size_t>(c->ncell), &t.density)) != DSMC_OK) return rc;
+    if ((rc = alloc_zero(c, static_cast<size_t>(c->nhcell), &t.horizon)) != DSMC_OK) return rc;
+    if (c->nhist > 0 && (rc = alloc_zero(c, static_cast<size_t>(c->nhist), &t.speed_hist)) != DSMC_OK)
+        return rc;
+    t.stats = c->stats;
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(c->stats, 0, dsmc::kStatCount * sizeof(unsigned long long), c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->ready = true;
+    return DSMC_OK;
+}
+
+int dsmc_enable_particle_outputs(dsmc_ctx *c, int64_t n) {
+    if (!c || n < 0) return DSMC_ERR_INVALID;
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    free_outputs(c);
+    if (n == 0) return DSMC_OK;
+    DSMC_CUDA_TRY(c, cudaMalloc(&c->outputs[0], static_cast<size_t>(n) * 9 * sizeof(double)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&c->outputs[1], static_cast<size_t>(n) * sizeof(int)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&c->outputs[2], static_cast<size_t>(n) * sizeof(long long)));
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(c->outputs[0], 0, static_cast<size_t>(n) * 9 * sizeof(double), c->stream));
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(c->outputs[1], 0, static_cast<size_t>(n) * sizeof(int), c->stream));
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(c->outputs[2], 0, static_cast<size_t>(n) * sizeof(long long), c->stream));
+    c->t.ttime = static_cast<double *>(c->outputs[0]);
+    c->t.fate = static_cast<int *>(c->outputs[1]);
+    c->t.steps = static_cast<long long *>(c->outputs[2]);
+    c->t.out_cap = n;
+    return DSMC_OK;
+}
+
+int dsmc_zero(dsmc_ctx *c) {
+    if (!c) return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "dsmc_zero before dsmc_setup");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(c->t.density, 0, c->ncell * sizeof(unsigned long long), c->stream));
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(c->t.horizon, 0, c->nhcell * sizeof(unsigned long long), c->stream));
+    if (c->t.speed_hist)
+        DSMC_CUDA_TRY(c, cudaMemsetAsync(c->t.speed_hist, 0, c->nhist * sizeof(unsigned long long), c->stream));
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(c->stats, 0, dsmc::kStatCount * sizeof(unsigned long long), c->stream));
+    if (c->t.out_cap > 0) {
+        DSMC_CUDA_TRY(c, cudaMemsetAsync(c->t.ttime, 0, c->t.out_cap * 9 * sizeof(double), c->stream));
+        DSMC_CUDA_TRY(c, cudaMemsetAsync(c->t.fate, 0, c->t.out_cap * sizeof(int), c->stream));
+        DSMC_CUDA_TRY(c, cudaMemsetAsync(c->t.steps, 0, c->t.out_cap * sizeof(long long), c->stream));
+    }
+    return DSMC_OK;
+}
+
+int dsmc_run(dsmc_ctx *c, int path, int64_t pid_begin, int64_t n) {
+    if (!c) return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "dsmc_run before dsmc_setup");
+    if (n < 0 || pid_begin < 0 || pid_begin + n > (int64_t(1) << 32))
+        return fail(c, DSMC_ERR_INVALID, "particle ids must lie in [0, 2^32)");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    c->t.out_base = pid_begin;
+    switch (path) {
+        case DSMC_PATH_PLAIN_FP64:
+            DSMC_CUDA_TRY(c, dsmc::launch_plain_fp64(c->params, c->t, pid_begin, n, c->num_sms, c->stream));
+            return DSMC_OK;
+        case DSMC_PATH_FAST_FP32:
+        case DSMC_PATH_FAST_FP64: {
+            if (!c->fast) {
+                c->fast = new (std::nothrow) dsmc::FastEngine();
+                if (!c->fast) return fail(c, DSMC_ERR_NO_MEMORY, "host allocation failed");
+            }
+            cudaError_t e = c->fast->run(c->params, c->t, path == DSMC_PATH_FAST_FP64, pid_begin, n,
+                                         c->num_sms, c->stream);
+            if (e != cudaSuccess)
+                return fail(c, e == cudaErrorMemoryAllocation ? DSMC_ERR_NO_MEMORY : DSMC_ERR_CUDA,
+                            "fast path: %s", cudaGetErrorString(e));
+            return DSMC_OK;
+        }
+        default:
+            return fail(c, DSMC_ERR_INVALID, "unknown path %d", path);
+    }
+}
+
+int dsmc_sync(dsmc_ctx *c) {
+    if (!c) return DSMC_ERR_INVALID;
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_get_density(dsmc_ctx *c, uint64_t *out) {
+    if (!c || !out) return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "no problem set up");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(out, c->t.density, c->ncell * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_get_horizon(dsmc_ctx *c, uint64_t *out) {
+    if (!c || !out) return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "no problem set up");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(out, c->t.horizon, c->nhcell * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_get_speed_hist(dsmc_ctx *c, uint64_t *out) {
+    if (!c || !out) return DSMC_ERR_INVALID;
+    if (!c->ready || !c->t.speed_hist) return fail(c, DSMC_ERR_STATE, "no speed histogram");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(out, c->t.speed_hist, c->nhist * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_get_stats(dsmc_ctx *c, dsmc_stats *out) {
+    if (!c || !out) return DSMC_ERR_INVALID;
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    unsigned long long s[dsmc::kStatCount];
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(s, c->stats, sizeof s, cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    out->total_steps = static_cast<int64_t>(s[dsmc::kStatSteps]);
+    out->n_escaped = static_cast<int64_t>(s[dsmc::kStatEscaped]);
+    out->n_collisions = static_cast<int64_t>(s[dsmc::kStatCollisions]);
+    out->n_bound_launch = static_cast<int64_t>(s[dsmc::kStatBound]);
+    out->n_finished = static_cast<int64_t>(s[dsmc::kStatFinished]);
+    out->n_drift_flagged = static_cast<int64_t>(s[dsmc::kStatDrift]);
+    return DSMC_OK;
+}
+
+int dsmc_get_particle_outputs(dsmc_ctx *c, int64_t n, double *ttime, int32_t *fate,
+                              int64_t *steps) {
+    if (!c || n < 0) return DSMC_ERR_INVALID;
+    if (n > c->t.out_cap) return fail(c, DSMC_ERR_INVALID, "n exceeds the per-particle capacity");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    if (n == 0) return DSMC_OK;
+    if (ttime)
+        for (int r = 0; r < 9; r++)
+            DSMC_CUDA_TRY(c, cudaMemcpyAsync(ttime + r * n, c->t.ttime + r * c->t.out_cap, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (fate) DSMC_CUDA_TRY(c, cudaMemcpyAsync(fate, c->t.fate, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    if (steps) DSMC_CUDA_TRY(c, cudaMemcpyAsync(steps, c->t.steps, n * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_density_device(dsmc_ctx *c, uint64_t **dev_ptr, int64_t *ncell) {
+    if (!c || !dev_ptr || !ncell) return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "no problem set up");
+    *dev_ptr = reinterpret_cast<uint64_t *>(c->t.density);
+    *ncell = c->ncell;
+    return DSMC_OK;
+}
+
+int dsmc_horizon_device(dsmc_ctx *c, uint64_t **dev_ptr, int64_t *ncell) {
+    if (!c || !dev_ptr || !ncell) return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "no problem set up");
+    *dev_ptr = reinterpret_cast<uint64_t *>(c->t.horizon);
+    *ncell = c->nhcell;
+    return DSMC_OK;
+}
+
+namespace {
+
+// Temporary device buffers of one fit call, freed on every exit path.
+struct FitBuffers {
+    void *p[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    ~FitBuffers() { for (void *q : p) if (q) cudaFree(q); }
+};
+
+int fit_common(dsmc_ctx *c, FitBuffers &b, int64_t ncell, size_t in_bytes, const void *in_host,
+               const int32_t *counts) {
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[0], in_bytes));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(b.p[0], in_host, in_bytes, cudaMemcpyHostToDevice, c->stream));
+    if (counts) {
+        DSMC_CUDA_TRY(c, cudaMalloc(&b.p[1], ncell * sizeof(int)));
+        DSMC_CUDA_TRY(c, cudaMemcpyAsync(b.p[1], counts, ncell * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    }
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[2], ncell * DSMC_CDF_STRIDE * sizeof(double)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[3], ncell * 4 * sizeof(double)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[4], ncell * sizeof(double)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[5], ncell * sizeof(int)));
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(b.p[3], 0, ncell * 4 * sizeof(double), c->stream));
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(b.p[4], 0, ncell * sizeof(double), c->stream));
+    return DSMC_OK;
+}
+
+int fit_finish(dsmc_ctx *c, FitBuffers &b, int64_t ncell, double *coef, double *box,
+               double *total, int32_t *valid) {
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(coef, b.p[2], ncell * DSMC_CDF_STRIDE * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(box, b.p[3], ncell * 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(total, b.p[4], ncell * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(valid, b.p[5], ncell * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+}  // namespace
+
+int dsmc_fit_cdf_samples_host(dsmc_ctx *c, int64_t ncell, int max_per_cell, const double *speeds,
+                              const int32_t *counts, int degree, double *coef, double *box,
+                              double *total, int32_t *valid) {
+    if (!c || !speeds || !counts || !coef || !box || !total || !valid) return DSMC_ERR_INVALID;
+    if (ncell <= 0 || ncell > (1 << 30) || max_per_cell < 1 || max_per_cell > 64 || degree < 0 ||
+        degree > DSMC_CDF_MAX_DEGREE)
+        return fail(c, DSMC_ERR_INVALID, "fit: bad sizes");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    FitBuffers b;
+    if ((rc = fit_common(c, b, ncell, ncell * max_per_cell * sizeof(double), speeds, counts)) != DSMC_OK)
+        return rc;
+    DSMC_CUDA_TRY(c, dsmc::launch_fit_samples(static_cast<int>(ncell), max_per_cell,
+                                              static_cast<const double *>(b.p[0]),
+                                              static_cast<const int *>(b.p[1]), degree,
+                                              static_cast<double *>(b.p[2]), static_cast<double *>(b.p[3]),
+                                              static_cast<double *>(b.p[4]), static_cast<int *>(b.p[5]),
+                                              c->stream));
+    return fit_finish(c, b, ncell, coef, box, total, valid);
+}
+
+int dsmc_fit_cdf_hist_host(dsmc_ctx *c, int64_t ncell, int nbins, double bin_width,
+                           const uint64_t *hist, int degree, double *coef, double *box,
+                           double *total, int32_t *valid) {
+    if (!c || !hist || !coef || !box || !total || !valid) return DSMC_ERR_INVALID;
+    if (ncell <= 0 || ncell > (1 << 30) || nbins < 1 || nbins > 64 || !(bin_width > 0.0) ||
+        degree < 0 || degree > DSMC_CDF_MAX_DEGREE)
+        return fail(c, DSMC_ERR_INVALID, "fit: bad sizes");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    FitBuffers b;
+    if ((rc = fit_common(c, b, ncell, ncell * nbins * sizeof(uint64_t), hist, nullptr)) != DSMC_OK)
+        return rc;
+    DSMC_CUDA_TRY(c, dsmc::launch_fit_hist(static_cast<int>(ncell), nbins, bin_width,
+                                           static_cast<const unsigned long long *>(b.p[0]), degree,
+                                           static_cast<double *>(b.p[2]), static_cast<double *>(b.p[3]),
+                                           static_cast<double *>(b.p[4]), static_cast<int *>(b.p[5]),
+                                           c->stream));
+    return fit_finish(c, b, ncell, coef, box, total, valid);
+}
+
+int dsmc_velocity_record(dsmc_ctx *c, int64_t n, int per_bucket, int64_t total_cap,
+                         double *v_out, int32_t *td, int32_t *fd, int32_t *ht, int64_t *n_out) {
+    if (!c || !v_out || !td || !fd || !ht || !n_out || n < 0 || per_bucket < 1 || total_cap < 0)
+        return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "dsmc_velocity_record before dsmc_setup");
+    if (c->params.runner != DSMC_RUNNER_BALLISTIC)
+        return fail(c, DSMC_ERR_INVALID, "the velocity record belongs to the ballistic runner");
+    if (n > (int64_t(1) << 32)) return fail(c, DSMC_ERR_INVALID, "particle ids must lie in [0, 2^32)");
+    *n_out = 0;
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    const int hd = c->params.hd;
+    const long long nb = static_cast<long long>(c->params.ftd) * hd;
+    // Chunk of particles whose per-bucket counter rows fit in ~64 MB.
+    long long chunk = (64ll << 20) / (4 * nb);
+    chunk = chunk < 256 ? 256 : chunk;
+    if (chunk > n) chunk = n > 0 ? n : 1;
+    struct Bufs {
+        void *p[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+        ~Bufs() { for (void *q : p) if (q) cudaFree(q); }
+    } b;
+    const long long slots = nb * per_bucket;
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[0], chunk * nb * sizeof(int)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[1], nb * sizeof(int)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[2], slots * 3 * sizeof(double)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[3], slots * sizeof(int)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[4], slots * sizeof(unsigned long long)));
+    DSMC_CUDA_TRY(c, cudaMemsetAsync(b.p[1], 0, nb * sizeof(int), c->stream));
+    dsmc::RecordArgs ra{};
+    ra.rows = static_cast<int *>(b.p[0]);
+    ra.cap = per_bucket;
+    ra.rec_v = static_cast<double *>(b.p[2]);
+    ra.rec_fd = static_cast<int *>(b.p[3]);
+    ra.rec_key = static_cast<unsigned long long *>(b.p[4]);
+    std::vector<int> filled(static_cast<size_t>(nb), 0);
+    for (long long p0 = 0; p0 < n; p0 += chunk) {
+        const long long kc = n - p0 < chunk ? n - p0 : chunk;
+        ra.row_base = p0;
+        DSMC_CUDA_TRY(c, cudaMemsetAsync(ra.rows, 0, kc * nb * sizeof(int), c->stream));
+        DSMC_CUDA_TRY(c, dsmc::launch_plain_record(c->params, c->t, p0, kc, ra,
+                                                   static_cast<int *>(b.p[1]), c->num_sms, c->stream));
+        DSMC_CUDA_TRY(c, cudaMemcpyAsync(filled.data(), b.p[1], nb * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        long long have = 0;
+        bool all_full = true;
+        for (long long k = 0; k < nb; k++) {
+            have += filled[k] < per_bucket ? filled[k] : per_bucket;
+            all_full = all_full && filled[k] >= per_bucket;
+        }
+        if (all_full || have >= total_cap) break;
+    }
+    std::vector<double> hv(static_cast<size_t>(slots) * 3);
+    std::vector<int> hfd(static_cast<size_t>(slots));
+    std::vector<unsigned long long> hkey(static_cast<size_t>(slots));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(hv.data(), b.p[2], slots * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(hfd.data(), b.p[3], slots * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(hkey.data(), b.p[4], slots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    // Records in global (pid, step) order, as the reference's single-thread run appends them.
+    std::vector<std::pair<unsigned long long, long long>> order;
+    for (long long k = 0; k < nb; k++) {
+        const int m = filled[k] < per_bucket ? filled[k] : per_bucket;
+        for (int j = 0; j < m; j++) order.emplace_back(hkey[k * per_bucket + j], k * per_bucket + j);
+    }
+    std::sort(order.begin(), order.end());
+    const long long nrec = static_cast<long long>(order.size()) < total_cap
+                               ? static_cast<long long>(order.size()) : total_cap;
+    for (long long i = 0; i < nrec; i++) {
+        const long long s = order[i].second, bucket = s / per_bucket;
+        v_out[3 * i] = hv[3 * s];
+        v_out[3 * i + 1] = hv[3 * s + 1];
+        v_out[3 * i + 2] = hv[3 * s + 2];
+        td[i] = static_cast<int32_t>(bucket / hd);
+        ht[i] = static_cast<int32_t>(bucket % hd);
+        fd[i] = hfd[s];
+    }
+    *n_out = nrec;
+    return DSMC_OK;
+}
+
+int dsmc_solve_host(dsmc_ctx *c, int path, const dsmc_params *p, const dsmc_surface *s,
+                    const dsmc_collision *col, int64_t n, uint64_t *density_fx,
+                    uint64_t *horizon_fx, dsmc_stats *stats) {
+    int rc = dsmc_setup(c, p, s, col);
+    if (rc == DSMC_OK) rc = dsmc_run(c, path, 0, n);
+    if (rc == DSMC_OK && density_fx) rc = dsmc_get_density(c, density_fx);
+    if (rc == DSMC_OK && horizon_fx) rc = dsmc_get_horizon(c, horizon_fx);
+    if (rc == DSMC_OK && stats) rc = dsmc_get_stats(c, stats);
+    if (rc == DSMC_OK) rc = dsmc_sync(c);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,26 @@
+// dsmc_kernels.h - host-side launchers of the DSMC kernels (internal to the library).
+#pragma once
+
+#include "dsmc_device.cuh"
+
+namespace dsmc {
+
+// Plain FP64 path: one thread per particle for its whole life (kernel_plain.cu).
+cudaError_t launch_plain_fp64(const dsmc_params &p, const DevTables &t, long long pid_begin,
+                              long long n, int num_sms, cudaStream_t stream);
+
+// Velocity-record replay of particles [pid_begin, pid_begin + n): count pass, per-bucket scan
+// (filled[b] holds the records each bucket already has and is advanced), record pass.
+cudaError_t launch_plain_record(const dsmc_params &p, const DevTables &t, long long pid_begin,
+                                long long n, const RecordArgs &ra, int *filled, int num_sms,
+                                cudaStream_t stream);
+
+// Per-cell FP64 CDF fits (kernel_fit.cu).
+cudaError_t launch_fit_samples(int ncell, int max_per_cell, const double *speeds,
+                               const int *counts, int degree, double *coef, double *box,
+                               double *total, int *valid, cudaStream_t stream);
+cudaError_t launch_fit_hist(int ncell, int nbins, double bin_width, const unsigned long long *hist,
+                            int degree, double *coef, double *box, double *total, int *valid,
+                            cudaStream_t stream);
+
+}  // namespace dsmc

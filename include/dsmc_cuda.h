@@ -1,0 +1,170 @@
+/* dsmc_cuda.h - the C ABI between the DSMC host code and the sm_100a kernels.
+ *
+ * The reference runs its particle loops inside run_ballistic (src/dsmc/ballistic.c:35-36) and
+ * run_advanced (src/dsmc/advanced.c:119-121), declared only as `extern` in src/main.c:18-23, with
+ * OpenMP threads over particles. This header is the seam that replaces those loops: the drop-in
+ * runners (same signatures, include/dsmc_runners.h) and the CLI call these functions, and every
+ * one is plain C: pointers, sizes and status codes, no exceptions and no C++ or torch types.
+ *
+ * Conventions
+ *   - Every function returns int status: DSMC_OK (0) or a negative dsmc_status.
+ *   - A context owns one device, one stream and the device buffers of one problem. A context is
+ *     not thread-safe; use one per host thread. Several contexts may share a device.
+ *   - Functions named *_host take host pointers and copy inside the call. Functions without that
+ *     suffix work on device-resident state and are asynchronous on the context stream.
+ *   - There is no CPU fallback: without a usable CUDA device, dsmc_ctx_create fails with
+ *     DSMC_ERR_NO_DEVICE.
+ */
+#ifndef DSMC_CUDA_H
+#define DSMC_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "dsmc_params.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum dsmc_status {
+    DSMC_OK = 0,
+    DSMC_ERR_INVALID = -1,      /* bad argument or inconsistent sizes */
+    DSMC_ERR_CUDA = -2,         /* a CUDA runtime call failed (see dsmc_last_error) */
+    DSMC_ERR_NO_DEVICE = -3,    /* no CUDA device, or the device index is out of range */
+    DSMC_ERR_NO_MEMORY = -4,    /* device or pinned host allocation failed */
+    DSMC_ERR_STATE = -5,        /* call out of order (e.g. run before setup) */
+    DSMC_ERR_BUDGET = -6,       /* admission refused: the request exceeds the memory budget */
+    DSMC_ERR_IO = -7            /* file could not be read or written */
+};
+
+/* ---------------------------------------------------------------------------------------- */
+/* Host-side set-up helpers (no device needed).                                              */
+
+/* Reference-model parameters exactly as the reference runners fill them:
+ * runner DSMC_RUNNER_BALLISTIC -> src/dsmc/ballistic.c:49-67 (100 uniform shells, dt 5 s);
+ * runner DSMC_RUNNER_ADVANCED  -> src/dsmc/advanced.c:131-152 (50 exponential shells, dt 0.5 s).
+ * ftd/ffd come from the temperature file. */
+int dsmc_params_reference(dsmc_params *p, int runner, int ftd, int ffd);
+
+/* Config-model parameters: body radius [m], GM [m^3/s^2], shells hd (exponential, to 10 R),
+ * 36 x 72 angular grid, dt 2 s, 20,000-step life cap, photolysis lifetime 2.6e5 s, H2O
+ * m = 2.99e-26 kg, sun on +x (sub-solar longitude pi/2). */
+int dsmc_params_config(dsmc_params *p, int runner, double Radii, double GM, int hd,
+                       uint64_t seed);
+
+/* Icosphere of 20 * 4^nlevel faces (1280 at nlevel 3, 642 vertices), built by midpoint
+ * subdivision of the icosahedron with faces kept in subdivision order (face index =
+ * base * 4^nlevel + child path). Fills face_verts [nface][3][3], base_centroid [20][3] and
+ * split_planes [20 * (4^nlevel - 1) / 3][3][3] (corner-cut planes used to locate a point). */
+int dsmc_icosphere_nface(int nlevel);
+int dsmc_icosphere_nnode(int nlevel);
+int dsmc_icosphere_build(int nlevel, double *face_verts, double *base_centroid,
+                         double *split_planes);
+/* Face containing unit direction p, by descending the subdivision tree. */
+int dsmc_icosphere_locate(int nlevel, const double *base_centroid, const double *split_planes,
+                          const double p[3]);
+
+/* Synthetic temperature field T = max(T_floor, T_ss * cos(z)^(1/4)), z the solar zenith:
+ * per face at the face centroid, or per latitude-longitude cell centre. */
+int dsmc_face_temperature(int nface, const double *face_verts, const double sun[3],
+                          double T_ss, double T_floor, double *face_T);
+int dsmc_latlon_temperature(int ftd, int ffd, const double sun[3], double T_ss,
+                            double T_floor, double *T_map);
+
+/* Antoine sublimation flux of H2O [molecules m^-2 s^-1] at T (vapour pressure of
+ * src/thermal/thermal_model.c:50-55 with the constants of :33-38, divided by sqrt(2 pi m k T)). */
+double dsmc_sublimation_flux(double T, double mmass_kg);
+
+/* Launch-face CDF weighted by face area x sublimation flux. Returns the total production rate
+ * for a unit-radius body [molecules/s per m^2 of R^2] in *rate_per_R2. */
+int dsmc_source_cdf(int nface, const double *face_verts, const double *face_T, double mmass_kg,
+                    double *face_cdf, double *rate_per_R2);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Device contexts.                                                                          */
+
+typedef struct dsmc_ctx dsmc_ctx;
+
+/* Solve paths. PLAIN_FP64 is the straight port: one thread per particle for its whole life,
+ * the reference's FP64 arithmetic without FMA contraction, one atomic per deposited step.
+ * FAST_FP32 keeps resident particle slots that refill from a work queue, pushes in FP32 with
+ * two-sum compensated positions and velocities, tracks cells by comparisons, and aggregates
+ * deposits in registers. FAST_FP64 is the same resident-slot engine with FP64 arithmetic. */
+enum dsmc_path { DSMC_PATH_PLAIN_FP64 = 0, DSMC_PATH_FAST_FP32 = 1, DSMC_PATH_FAST_FP64 = 2 };
+
+typedef struct dsmc_stats {
+    int64_t total_steps;      /* Verlet steps executed */
+    int64_t n_escaped;
+    int64_t n_collisions;
+    int64_t n_bound_launch;   /* config model: launches with negative energy */
+    int64_t n_finished;       /* particles whose life ended */
+    int64_t n_drift_flagged;  /* trajectories whose energy drift exceeded the guard */
+} dsmc_stats;
+
+const char *dsmc_status_string(int status);
+/* Text of the last error on this context (or of the last failed dsmc_ctx_create). */
+const char *dsmc_last_error(const dsmc_ctx *ctx);
+
+int dsmc_ctx_create(int device, dsmc_ctx **out);
+int dsmc_ctx_destroy(dsmc_ctx *ctx);
+/* Run on the caller's stream (a cudaStream_t passed as void*), or NULL for the context's own. */
+int dsmc_ctx_set_stream(dsmc_ctx *ctx, void *stream);
+
+/* Upload one problem: parameters, surface and (advanced runner) collision tables. Allocates the
+ * density [hd][ftd][ffd] and horizon [ftd][ffd] fixed-point grids and zeroes them. */
+int dsmc_setup(dsmc_ctx *ctx, const dsmc_params *p, const dsmc_surface *surf,
+               const dsmc_collision *col);
+/* Allocate per-particle outputs for up to n particles (ttime rows, fate, steps); 0 frees them. */
+int dsmc_enable_particle_outputs(dsmc_ctx *ctx, int64_t n);
+/* Zero grids, per-particle outputs and statistics. */
+int dsmc_zero(dsmc_ctx *ctx);
+/* Solve particles [pid_begin, pid_begin + n) on the device, adding into the grids. Async. */
+int dsmc_run(dsmc_ctx *ctx, int path, int64_t pid_begin, int64_t n);
+int dsmc_sync(dsmc_ctx *ctx);
+
+/* Results (synchronous copies to host memory). */
+int dsmc_get_density(dsmc_ctx *ctx, uint64_t *density_fx);
+int dsmc_get_horizon(dsmc_ctx *ctx, uint64_t *horizon_fx);
+int dsmc_get_stats(dsmc_ctx *ctx, dsmc_stats *out);
+/* Per-cell speed histogram [hd*ftd*ffd][n_speed_bins] (when params.n_speed_bins > 0). */
+int dsmc_get_speed_hist(dsmc_ctx *ctx, uint64_t *hist);
+/* ttime [9][n], fate [n], steps [n] for the particles of the last runs, indexed pid - pid_begin
+ * of the run that produced them. Any pointer may be NULL. */
+int dsmc_get_particle_outputs(dsmc_ctx *ctx, int64_t n, double *ttime, int32_t *fate,
+                              int64_t *steps);
+/* Device address of the fixed-point density grid and its length in cells, for collectives. */
+int dsmc_density_device(dsmc_ctx *ctx, uint64_t **dev_ptr, int64_t *ncell);
+int dsmc_horizon_device(dsmc_ctx *ctx, uint64_t **dev_ptr, int64_t *ncell);
+
+/* FP64 fits of per-cell collision-partner speed CDFs, computed on the device; host buffers in
+ * and out. From speed samples (the reference's build_poly_fits, src/dsmc/advanced.c:32-117):
+ * speeds [ncell][max_per_cell] with counts [ncell] (max_per_cell <= 64). From speed histograms
+ * (config model): hist [ncell][nbins] of width bin_width. Outputs coef [ncell][DSMC_CDF_STRIDE],
+ * box [ncell][4], total [ncell] and valid [ncell], ready for a dsmc_collision. */
+int dsmc_fit_cdf_samples_host(dsmc_ctx *ctx, int64_t ncell, int max_per_cell,
+                              const double *speeds, const int32_t *counts, int degree,
+                              double *coef, double *box, double *total, int32_t *valid);
+int dsmc_fit_cdf_hist_host(dsmc_ctx *ctx, int64_t ncell, int nbins, double bin_width,
+                           const uint64_t *hist, int degree, double *coef, double *box,
+                           double *total, int32_t *valid);
+
+/* Velocity record of the ballistic runner (src/dsmc/ballistic.c:216-232): for each
+ * (latitude row, shell) bucket, the first per_bucket visits in (particle id, step) order, i.e.
+ * the records the reference keeps in a one-thread run, at most total_cap records in that order.
+ * Replays particles [0, n) of the problem set up on ctx in chunks (count pass, per-bucket scan,
+ * record pass) and stops once every bucket or the total is full. The grids are not touched.
+ * v_out [total_cap][3], td/fd/ht [total_cap]; *n_out receives the count. */
+int dsmc_velocity_record(dsmc_ctx *ctx, int64_t n, int per_bucket, int64_t total_cap,
+                         double *v_out, int32_t *td, int32_t *fd, int32_t *ht, int64_t *n_out);
+
+/* Host-buffer solve: set-up, n particles from pid 0, results copied back into host buffers.
+ * This is the one call a plugin makes; density_fx [hd*ftd*ffd] and horizon_fx [ftd*ffd] may be
+ * NULL. */
+int dsmc_solve_host(dsmc_ctx *ctx, int path, const dsmc_params *p, const dsmc_surface *surf,
+                    const dsmc_collision *col, int64_t n, uint64_t *density_fx,
+                    uint64_t *horizon_fx, dsmc_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSMC_CUDA_H */

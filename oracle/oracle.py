@@ -1,0 +1,163 @@
+"""ctypes wrapper of the CPU oracle (oracle/liboracle.so) - TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker; the
+product (dsmc_suite_b200/) never imports it. build() compiles oracle/dsmc_oracle.c with gcc, and
+build_ref() compiles the reference's own sources into oracle/_ref/ when the reference tree is
+present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_DIR = HERE / "_ref"
+RNG_RAND_R, RNG_PHILOX = 0, 1
+
+
+def build(ref_root: str | None = None) -> None:
+    """Build liboracle.so; also oracle/_ref when the reference sources exist."""
+    env = dict(os.environ)
+    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True, env=env)
+    ref = ref_root or os.environ.get("DSMC_REFERENCE_ROOT", "/root/reference")
+    if Path(ref, "src", "dsmc", "ballistic.c").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True, env=env)
+
+
+class VTable(C.Structure):
+    _fields_ = [("temps", C.c_double * 23), ("speeds", (C.c_double * 1000) * 23),
+                ("count", C.c_int * 23)]
+
+
+class Outputs(C.Structure):
+    _fields_ = [
+        ("density_f64", C.POINTER(C.c_double)), ("density_fx", C.POINTER(C.c_uint64)),
+        ("horizon_f64", C.POINTER(C.c_double)), ("horizon_fx", C.POINTER(C.c_uint64)),
+        ("ttime", C.POINTER(C.c_double)), ("fate", C.POINTER(C.c_int32)),
+        ("steps", C.POINTER(C.c_int64)), ("speed_hist", C.POINTER(C.c_uint64)),
+        ("v_record", C.POINTER(C.c_double)), ("v_td", C.POINTER(C.c_int32)),
+        ("v_fd", C.POINTER(C.c_int32)), ("v_ht", C.POINTER(C.c_int32)),
+        ("v_count_nn", C.POINTER(C.c_int32)), ("v_cap", C.c_int64), ("n_records", C.c_int64),
+        ("total_steps", C.c_int64), ("n_escaped", C.c_int64), ("n_collisions", C.c_int64),
+        ("n_bound_launch", C.c_int64),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        from dsmc_suite_b200 import _native as N
+        L = C.CDLL(str(LIB))
+        D = C.POINTER(C.c_double)
+        L.or_run.restype = C.c_int
+        L.or_run.argtypes = [C.POINTER(N.Params), C.POINTER(N.Surface), C.POINTER(N.Collision),
+                             C.POINTER(VTable), C.c_int, C.c_uint, C.c_int64, C.c_int64, C.c_int,
+                             C.POINTER(Outputs)]
+        L.or_philox4x32.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32)]
+        L.or_verlet_step.restype = C.c_int
+        L.or_verlet_step.argtypes = [D, D, D, C.c_double, C.c_double, C.c_double, C.c_double, D]
+        L.or_spherical_to_index.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int,
+                                            C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.or_exp_ht_index.restype = C.c_int
+        L.or_exp_ht_index.argtypes = [C.c_double] * 5
+        L.or_velocity_table_init.argtypes = [C.POINTER(VTable), C.c_double, C.c_double, C.c_double]
+        L.or_velocity_sample_word.restype = C.c_double
+        L.or_velocity_sample_word.argtypes = [C.POINTER(VTable), C.c_double, C.c_uint32]
+        L.or_cdf_sample.restype = C.c_double
+        L.or_cdf_sample.argtypes = [D, D, C.c_double, C.c_int, C.c_double]
+        L.or_polyfit.restype = C.c_int
+        L.or_polyfit.argtypes = [D, D, C.c_int, C.c_int, D]
+        L.or_fit_cell_from_samples.restype = C.c_int
+        L.or_fit_cell_from_samples.argtypes = [D, C.c_int, C.c_int, D, D, D]
+        L.or_fit_cell_from_hist.restype = C.c_int
+        L.or_fit_cell_from_hist.argtypes = [C.POINTER(C.c_uint64), C.c_int, C.c_double, C.c_int,
+                                            D, D, D]
+        L.or_locate_face.restype = C.c_int
+        L.or_locate_face.argtypes = [C.POINTER(N.Surface), D]
+        _lib = L
+    return _lib
+
+
+def _p(a, t=C.c_double):
+    if a is None:
+        return C.POINTER(t)()
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def vtable(mmass=18e-3, mole=6.02e23, k_B=1.38e-23) -> VTable:
+    vt = VTable()
+    lib().or_velocity_table_init(C.byref(vt), mmass, mole, k_B)
+    return vt
+
+
+def philox(ctr, key) -> list[int]:
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().or_philox4x32(c, k, o)
+    return list(o)
+
+
+def run(params, surface, n: int, collision=None, rng: int = RNG_PHILOX, rr_seed: int = 67890,
+        pid_begin: int = 0, nthreads: int = 1, fixed: bool = True, f64: bool = False,
+        particles: bool = True, v_record: bool = False, speed_hist: bool = False) -> dict:
+    """Run the oracle over particles [pid_begin, pid_begin + n); returns numpy results.
+
+    surface / collision are dsmc_suite_b200._native.SurfaceInputs / CollisionInputs."""
+    p = params
+    ncell, nh = p.hd * p.ftd * p.ffd, p.ftd * p.ffd
+    o = Outputs()
+    res: dict = {}
+    keep = []
+
+    def arr(name, shape, dtype, field, ctype):
+        a = np.zeros(shape, dtype=dtype)
+        res[name] = a
+        keep.append(a)
+        setattr(o, field, _p(a, ctype))
+
+    if fixed:
+        arr("density", (p.hd, p.ftd, p.ffd), np.uint64, "density_fx", C.c_uint64)
+        arr("horizon", (p.ftd, p.ffd), np.uint64, "horizon_fx", C.c_uint64)
+    if f64:
+        arr("density_f64", (p.hd, p.ftd, p.ffd), np.float64, "density_f64", C.c_double)
+        arr("horizon_f64", (p.ftd, p.ffd), np.float64, "horizon_f64", C.c_double)
+    if particles:
+        arr("ttime", (9, n), np.float64, "ttime", C.c_double)
+        arr("fate", (n,), np.int32, "fate", C.c_int32)
+        arr("steps", (n,), np.int64, "steps", C.c_int64)
+    if speed_hist and p.n_speed_bins > 0:
+        arr("speed_hist", (ncell, p.n_speed_bins), np.uint64, "speed_hist", C.c_uint64)
+    if v_record:
+        cap = 100 * p.ftd * p.hd
+        arr("v_record", (cap, 3), np.float64, "v_record", C.c_double)
+        arr("v_td", (cap,), np.int32, "v_td", C.c_int32)
+        arr("v_fd", (cap,), np.int32, "v_fd", C.c_int32)
+        arr("v_ht", (cap,), np.int32, "v_ht", C.c_int32)
+        arr("v_count_nn", (p.ftd * p.hd,), np.int32, "v_count_nn", C.c_int32)
+        o.v_cap = cap
+    vt = vtable()
+    col = C.byref(collision.struct) if collision is not None else None
+    rc = lib().or_run(C.byref(p), C.byref(surface.struct), col, C.byref(vt), rng, rr_seed,
+                      pid_begin, n, nthreads, C.byref(o))
+    if rc != 0:
+        raise RuntimeError(f"or_run failed: {rc}")
+    for k in ("total_steps", "n_escaped", "n_collisions", "n_bound_launch", "n_records"):
+        res[k] = int(getattr(o, k))
+    if v_record:
+        k = res["n_records"]
+        for name in ("v_record", "v_td", "v_fd", "v_ht"):
+            res[name] = res[name][:k]
+    del nh
+    return res
