@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of the test-particle DSMC hot path on B200.
+
+Workload (one "step"): one complete solve of the config-1 ballistic problem - 1e8 H2O test
+particles per GPU on a Ceres-like body (R 470 km, GM 6.26e10), icosphere surface of 1280 faces with
+T = max(110 K, 235 K cos(z)^0.25), flux-weighted Maxwell-Boltzmann launch, Verlet dt 2 s, at most
+20,000 steps per particle, photolysis lifetime 2.6e5 s, 50 exponential shells to 10 R x 36 x 72.
+Every particle runs to the end of its life; the metric is particle-steps/s (Verlet steps
+executed, counted on the device).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One process per GPU (torchrun for N > 1); each rank solves its own 1e8 particles (weak scaling,
+disjoint particle ids) and the fixed-point grids are summed across ranks with one NCCL
+all-reduce inside the timed step. Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FLOPS_PER_STEP = 60   # algorithmic FP operations of one particle-step (verlet_step + cell +
+                      # photolysis + deposit of the reference algorithm)
+METRIC = "particle-steps/s"
+SEED = 20261203
+
+
+def args_parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--particles", type=float, default=1e8, help="particles per GPU per step")
+    ap.add_argument("--plain-particles", type=float, default=1e7,
+                    help="particles of the plain FP64 comparison solve (rank 0, N=1)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def config_problem(N):
+    p = N.params_config(N.RUNNER_BALLISTIC, 470e3, 6.26e10, 50, SEED)
+    ico = N.Icosphere(3)
+    S = N.SurfaceInputs(ico=ico, face_T=ico.face_temperature(T_ss=235.0, T_floor=110.0))
+    return p, S
+
+
+CONFIG = {"workload": "config-1 ballistic: Ceres-like body, icosphere 1280 faces, "
+                      "T=max(110,235cos^0.25), dt 2 s, <=20000 steps, tau 2.6e5 s, "
+                      "50 exp shells to 10R x 36 x 72",
+          "solver": "FAST_FP32 resident slots, two-sum compensated push",
+          "l2": "flushed before every timed step (256 MiB write)", "seed": SEED}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_rate(N, seconds: float, nthreads: int, n_hint: int | None = None):
+    """The oracle port (plain C, OpenMP over particles, Philox streams) on a bounded sample of
+    the same workload. Returns (steps/s, particles, steps, wall seconds)."""
+    from oracle import oracle as O
+    O.build()
+    p, S = config_problem(N)
+    if n_hint is None:
+        t0 = time.perf_counter()
+        r = O.run(p, S, 2000, nthreads=nthreads, particles=False)
+        rate = r["total_steps"] / (time.perf_counter() - t0)
+        per = r["total_steps"] / 2000
+        n_hint = max(2000, int(rate * seconds / per))
+    t0 = time.perf_counter()
+    r = O.run(p, S, n_hint, pid_begin=10_000_000, nthreads=nthreads, particles=False)
+    dt = time.perf_counter() - t0
+    return r["total_steps"] / dt, n_hint, r["total_steps"], dt
+
+
+def reference_binary_rate(seconds: float, nthreads: int):
+    """The unmodified reference binary (oracle/_ref/dsmc_suite, compiled from the reference's
+    own sources) on its own reference-model workload: `dsmc -n N -t cores` on the synthetic
+    36 x 72 map. Particle-steps = sum of flight_time / dt of its _ttime.dat (row 4), which
+    leaves out escaped particles as the reference records none for them."""
+    cli = ROOT / "oracle" / "_ref" / "dsmc_suite"
+    if not cli.exists():
+        return None
+    import tempfile
+    from dsmc_suite_b200 import _native as N
+    T = N.latlon_temperature(36, 72, T_ss=235.0, T_floor=110.0)
+    with tempfile.TemporaryDirectory() as d:
+        (Path(d) / "T.dat").write_text("36\n72\n" + "".join(f"{x:.17g}\n" for x in T.ravel()))
+        n = 2000
+        for _ in range(3):
+            t0 = time.perf_counter()
+            subprocess.run([str(cli), "dsmc", "-n", str(n), "-t", str(nthreads), "-T",
+                            str(Path(d) / "T.dat"), "-o", str(Path(d) / "r")], check=True,
+                           capture_output=True)
+            dt = time.perf_counter() - t0
+            tt = np.array((Path(d) / "r_ttime.dat").read_text().split(), dtype=np.float64)
+            steps = float(tt.reshape(5, n)[4].sum() / 5.0)
+            if dt > 0.3 * seconds:
+                break
+            n = int(n * min(20.0, max(1.5, seconds / max(dt, 1e-3))))
+    return {"value": steps / dt, "unit": METRIC, "cores": nthreads, "kind": "reference",
+            "sample": f"reference binary, its own physics (Ceres R 476.2 km, dt 5 s, 100 "
+                      f"uniform shells): dsmc -n {n} -t {nthreads}, {steps:.3e} steps in "
+                      f"{dt:.1f} s wall"}
+
+
+def run_reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from dsmc_suite_b200 import _native as N
+    cores = os.cpu_count() or 1
+    per_step = max(2.0, 90.0 / max(1, a.steps + a.warmup))
+    rate, n, steps, dt = cpu_oracle_rate(N, per_step, cores)
+    for _ in range(a.warmup - 1):
+        cpu_oracle_rate(N, per_step, cores, n)
+    rates, secs = [], []
+    for _ in range(a.steps):
+        r, _, s, d = cpu_oracle_rate(N, per_step, cores, n)
+        rates.append(r)
+        secs.append(d)
+    value = float(np.sum([r * d for r, d in zip(rates, secs)]) / np.sum(secs))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": float(np.mean(secs) * 1e3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": dict(CONFIG, solver="CPU oracle port of the reference "
+                                                "algorithm, OpenMP over particles"),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                             "sample": f"{n} particles of the same workload per step"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    refbin = reference_binary_rate(per_step, cores)
+    if refbin:
+        line["reference_binary"] = refbin
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = args_parse()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from dsmc_suite_b200 import _native as N, Context
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+    stream = torch.cuda.current_stream()
+    ctx = Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    p, S = config_problem(N)
+    n = int(a.particles)
+    pid0 = rank * n
+    ctx.setup(p, S)
+    ncell, nh = p.ncell, p.ftd * p.ffd
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    red = torch.zeros(ncell + nh, dtype=torch.int64, device="cuda") if world > 1 else None
+    L = N.lib()
+
+    def solve_step():
+        ctx.zero()
+        ctx.run(N.PATH_FAST_FP32, pid0, n)
+        if red is not None:
+            d_ptr = red.data_ptr()
+            N.check(L.dsmc_copy_grids_device(ctx.h, C_u64(d_ptr), C_u64(d_ptr + 8 * ncell)), "copy", ctx.h)
+            dist.all_reduce(red, op=dist.ReduceOp.SUM)
+
+    import ctypes
+    def C_u64(addr):
+        return ctypes.cast(ctypes.c_void_p(addr), ctypes.POINTER(ctypes.c_uint64))
+
+    for _ in range(a.warmup):
+        solve_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    steps_done, launches = 0, 0
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        for k in range(a.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            solve_step()
+            ev[k][1].record(stream)
+            st = ctx.stats()
+            steps_done += st["total_steps"]
+            li = (ctypes.c_int64(), ctypes.c_int64())
+            L.dsmc_get_launch_info(ctx.h, ctypes.byref(li[0]), ctypes.byref(li[1]))
+            launches += li[0].value
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    t_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    nslots = li[1].value
+    tot = torch.tensor([t_ms, float(steps_done)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        t_max = tot[:1].clone()
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        s_sum = tot[1:].clone()
+        dist.all_reduce(s_sum, op=dist.ReduceOp.SUM)
+        t_ms, steps_all = float(t_max.item()), float(s_sum.item())
+    else:
+        steps_all = float(steps_done)
+    value = steps_all / (t_ms * 1e-3)
+    per_rank_rate = steps_done / (t_ms * 1e-3)
+
+    # roofline of the push kernel: algorithmic FP ops / time against the measured FP32 FMA peak
+    peak = ctypes.c_double()
+    N.check(L.dsmc_measure_fma_peak(ctx.h, 0, ctypes.byref(peak)), "fma peak", ctx.h)
+    achieved = per_rank_rate * FLOPS_PER_STEP / 1e12
+    traffic = None
+    prof = ROOT / "profiles" / "fast_kernel_traffic.json"
+    if prof.exists() and launches:
+        tj = json.loads(prof.read_text())
+        # DRAM bytes per particle-step from the ncu capture, scaled to this run's launches
+        traffic = tj["dram_bytes_per_step"] * (steps_done / launches)
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
+                "peak_source": "measured in this run: FP32 FMA-chain kernel "
+                               "(dsmc_measure_fma_peak)",
+                "algorithmic_flops_per_step": FLOPS_PER_STEP}
+
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic", "config": dict(CONFIG, particles_per_gpu=n,
+                                               parallelism=f"particle shards x{world}"),
+            "particle_steps_per_step": steps_all / a.steps, "gpu_launches": launches,
+            "resident_slots": nslots, "clocks": clocks.summary(), "roofline": roofline}
+
+    if rank == 0 and world == 1:
+        # plain FP64 path (one thread per particle, the reference's arithmetic) on the same
+        # workload, for the FP32-batched vs plain-FP64 ratio
+        npl = int(a.plain_particles)
+        ctx.zero()
+        ctx.run(N.PATH_PLAIN_FP64, 0, 100000)
+        torch.cuda.synchronize()
+        ctx.zero()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        e0.record(stream)
+        ctx.run(N.PATH_PLAIN_FP64, 0, npl)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pst = ctx.stats()["total_steps"]
+        plain = pst / (e0.elapsed_time(e1) * 1e-3)
+        pk64 = ctypes.c_double()
+        N.check(L.dsmc_measure_fma_peak(ctx.h, 1, ctypes.byref(pk64)), "fma peak", ctx.h)
+        line["plain_fp64"] = {"value": plain, "unit": METRIC, "particles": npl,
+                              "fp64_fma_peak_tflops": pk64.value}
+        line["speedup_vs_plain_fp64"] = value / plain
+
+    if not a.no_e2e:
+        # end to end through the C ABI with host buffers: surface upload, solve, grid download
+        ctx2 = Context(local)
+        host = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+                for k, v in (("fv", S.ico.face_verts), ("bc", S.ico.base_centroid),
+                             ("sp", S.ico.split_planes), ("ft", S.face_T))}
+        ico_pinned = N.Icosphere.__new__(N.Icosphere)
+        ico_pinned.__dict__.update(S.ico.__dict__)
+        ico_pinned.face_verts, ico_pinned.base_centroid, ico_pinned.split_planes = \
+            host["fv"], host["bc"], host["sp"]
+        S_pin = N.SurfaceInputs(ico=ico_pinned, face_T=host["ft"])
+        den_h = torch.zeros(ncell, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+        hor_h = torch.zeros(nh, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+        stats = N.Stats()
+        pe = p.copy()
+        t0 = time.perf_counter()
+        N.check(L.dsmc_solve_host(ctx2.h, N.PATH_FAST_FP32, ctypes.byref(pe), ctypes.byref(S_pin.struct),
+                                  None, n, N.ptr(den_h, ctypes.c_uint64),
+                                  N.ptr(hor_h, ctypes.c_uint64), ctypes.byref(stats)),
+                "solve_host", ctx2.h)
+        dt = time.perf_counter() - t0
+        e2e_steps = float(stats.total_steps)
+        if world > 1:
+            agg = torch.tensor([dt, e2e_steps], dtype=torch.float64, device="cuda")
+            tmax, ssum = agg[:1].clone(), agg[1:].clone()
+            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+            dist.all_reduce(ssum, op=dist.ReduceOp.SUM)
+            dt, e2e_steps = float(tmax.item()), float(ssum.item())
+        h2d = sum(v.nbytes for v in host.values())
+        line["e2e"] = {"value": e2e_steps / dt, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": den_h.nbytes + hor_h.nbytes + ctypes.sizeof(stats),
+                       "api": "dsmc_solve_host (C ABI, pinned host buffers)",
+                       "seconds": dt}
+        ctx2.close()
+
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cores = os.cpu_count() or 1
+        rate, ncpu, scpu, dcpu = cpu_oracle_rate(N, a.cpu_seconds, cores)
+        line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "port",
+                                "sample": f"{ncpu} particles of the same workload, {scpu} "
+                                          f"particle-steps in {dcpu:.1f} s (oracle port, OpenMP)"}
+        refbin = reference_binary_rate(a.cpu_seconds, cores)
+        if refbin:
+            line["cpu_baseline"]["reference_binary"] = refbin
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -133,6 +133,11 @@ SIGNATURES = [
                                             _DP, _I32P]),
     ("dsmc_fit_cdf_hist_host", C.c_int, [_P, C.c_int64, C.c_int, C.c_double, _U64P, C.c_int, _DP,
                                          _DP, _DP, _I32P]),
+    ("dsmc_set_launch_shape", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("dsmc_get_launch_info", C.c_int, [_P, _I64P, _I64P]),
+    ("dsmc_measure_fma_peak", C.c_int, [_P, C.c_int, _DP]),
+    ("dsmc_copy_grids_device", C.c_int, [_P, _U64P, _U64P]),
+    ("dsmc_push_host", C.c_int, [_P, C.c_int, C.c_int64, C.c_int, _DP, _DP, _I32P, _I32P]),
     ("dsmc_velocity_record", C.c_int, [_P, C.c_int64, C.c_int, C.c_int64, _DP, _I32P, _I32P, _I32P,
                                        _I64P]),
     ("dsmc_solve_host", C.c_int, [_P, C.c_int, C.POINTER(Params), C.POINTER(Surface),

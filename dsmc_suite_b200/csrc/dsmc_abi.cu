@@ -31,6 +31,7 @@ struct dsmc_ctx {
     void *outputs[3] = {nullptr, nullptr, nullptr};  // ttime, fate, steps
     unsigned long long *stats = nullptr;
     dsmc::FastEngine *fast = nullptr;
+    long long last_launches = 0;
     char err[512] = {0};
 };
 
@@ -330,6 +331,7 @@ int dsmc_run(dsmc_ctx *c, int path, int64_t pid_begin, int64_t n) {
     switch (path) {
         case DSMC_PATH_PLAIN_FP64:
             DSMC_CUDA_TRY(c, dsmc::launch_plain_fp64(c->params, c->t, pid_begin, n, c->num_sms, c->stream));
+            c->last_launches = n > 0 ? 1 : 0;
             return DSMC_OK;
         case DSMC_PATH_FAST_FP32:
         case DSMC_PATH_FAST_FP64: {
@@ -339,6 +341,7 @@ int dsmc_run(dsmc_ctx *c, int path, int64_t pid_begin, int64_t n) {
             }
             cudaError_t e = c->fast->run(c->params, c->t, path == DSMC_PATH_FAST_FP64, pid_begin, n,
                                          c->num_sms, c->stream);
+            c->last_launches = c->fast->launches;
             if (e != cudaSuccess)
                 return fail(c, e == cudaErrorMemoryAllocation ? DSMC_ERR_NO_MEMORY : DSMC_ERR_CUDA,
                             "fast path: %s", cudaGetErrorString(e));
@@ -347,6 +350,57 @@ int dsmc_run(dsmc_ctx *c, int path, int64_t pid_begin, int64_t n) {
         default:
             return fail(c, DSMC_ERR_INVALID, "unknown path %d", path);
     }
+}
+
+int dsmc_set_launch_shape(dsmc_ctx *c, int block, int blocks_per_sm, int steps_per_launch,
+                          int launches_per_graph) {
+    if (!c) return DSMC_ERR_INVALID;
+    if (block < 32 || block > 1024 || block % 32 || blocks_per_sm < 0 || blocks_per_sm > 64 ||
+        steps_per_launch < 1 || steps_per_launch > (1 << 24) || launches_per_graph < 1 ||
+        launches_per_graph > 4096)
+        return fail(c, DSMC_ERR_INVALID, "launch shape out of range");
+    if (!c->fast) {
+        c->fast = new (std::nothrow) dsmc::FastEngine();
+        if (!c->fast) return fail(c, DSMC_ERR_NO_MEMORY, "host allocation failed");
+    }
+    c->fast->set_shape(block, blocks_per_sm, steps_per_launch, launches_per_graph);
+    return DSMC_OK;
+}
+
+int dsmc_measure_fma_peak(dsmc_ctx *c, int fp64, double *tflops) {
+    if (!c || !tflops) return DSMC_ERR_INVALID;
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    const int blocks = c->num_sms * 8, iters = fp64 ? 20000 : 40000;
+    void *scratch = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    DSMC_CUDA_TRY(c, cudaMalloc(&scratch, blocks * sizeof(double)));
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    float best_ms = 0.0f;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
+        e = cudaEventRecord(e0, c->stream);
+        if (e == cudaSuccess) e = dsmc::launch_fma_peak(fp64 != 0, scratch, blocks, iters, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess && rep > 0 && (best_ms == 0.0f || ms < best_ms)) best_ms = ms;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(scratch);
+    if (e != cudaSuccess) return fail(c, DSMC_ERR_CUDA, "fma peak: %s", cudaGetErrorString(e));
+    const double flops = 2.0 * 8.0 * iters * 256.0 * blocks;
+    *tflops = flops / (best_ms * 1e-3) / 1e12;
+    return DSMC_OK;
+}
+
+int dsmc_get_launch_info(dsmc_ctx *c, int64_t *launches, int64_t *nslots) {
+    if (!c || !launches || !nslots) return DSMC_ERR_INVALID;
+    *launches = c->last_launches;
+    *nslots = c->fast ? c->fast->slot_count() : 0;
+    return DSMC_OK;
 }
 
 int dsmc_sync(dsmc_ctx *c) {
@@ -416,6 +470,18 @@ int dsmc_get_particle_outputs(dsmc_ctx *c, int64_t n, double *ttime, int32_t *fa
     if (fate) DSMC_CUDA_TRY(c, cudaMemcpyAsync(fate, c->t.fate, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     if (steps) DSMC_CUDA_TRY(c, cudaMemcpyAsync(steps, c->t.steps, n * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
     DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_copy_grids_device(dsmc_ctx *c, uint64_t *density_dst, uint64_t *horizon_dst) {
+    if (!c) return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "no problem set up");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    if (density_dst)
+        DSMC_CUDA_TRY(c, cudaMemcpyAsync(density_dst, c->t.density, c->ncell * sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
+    if (horizon_dst)
+        DSMC_CUDA_TRY(c, cudaMemcpyAsync(horizon_dst, c->t.horizon, c->nhcell * sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
     return DSMC_OK;
 }
 
@@ -511,6 +577,40 @@ int dsmc_fit_cdf_hist_host(dsmc_ctx *c, int64_t ncell, int nbins, double bin_wid
                                            static_cast<double *>(b.p[4]), static_cast<int *>(b.p[5]),
                                            c->stream));
     return fit_finish(c, b, ncell, coef, box, total, valid);
+}
+
+int dsmc_push_host(dsmc_ctx *c, int path, int64_t n, int nsteps, double *pos, double *vel,
+                   int32_t *status, int32_t *steps_taken) {
+    if (!c || !pos || !vel || !status || n < 0 || nsteps < 0) return DSMC_ERR_INVALID;
+    if (!c->ready) return fail(c, DSMC_ERR_STATE, "dsmc_push_host before dsmc_setup");
+    if (path != DSMC_PATH_PLAIN_FP64 && path != DSMC_PATH_FAST_FP32 && path != DSMC_PATH_FAST_FP64)
+        return fail(c, DSMC_ERR_INVALID, "unknown path %d", path);
+    int rc = set_device(c);
+    if (rc != DSMC_OK || n == 0) return rc;
+    struct Bufs {
+        void *p[4] = {nullptr, nullptr, nullptr, nullptr};
+        ~Bufs() { for (void *q : p) if (q) cudaFree(q); }
+    } b;
+    const size_t vb = static_cast<size_t>(n) * 3 * sizeof(double);
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[0], vb));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[1], vb));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[2], n * sizeof(int)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[3], n * sizeof(int)));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(b.p[0], pos, vb, cudaMemcpyHostToDevice, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(b.p[1], vel, vb, cudaMemcpyHostToDevice, c->stream));
+    double *dp = static_cast<double *>(b.p[0]), *dv = static_cast<double *>(b.p[1]);
+    int *ds = static_cast<int *>(b.p[2]), *dt = static_cast<int *>(b.p[3]);
+    if (path == DSMC_PATH_FAST_FP32)
+        DSMC_CUDA_TRY(c, dsmc::launch_push_fp32(c->params, n, nsteps, dp, dv, ds, dt, c->stream));
+    else
+        DSMC_CUDA_TRY(c, dsmc::launch_push_fp64(c->params, n, nsteps, dp, dv, ds, dt, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(pos, dp, vb, cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(vel, dv, vb, cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(status, ds, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    if (steps_taken)
+        DSMC_CUDA_TRY(c, cudaMemcpyAsync(steps_taken, dt, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
 }
 
 int dsmc_velocity_record(dsmc_ctx *c, int64_t n, int per_bucket, int64_t total_cap,

@@ -15,6 +15,15 @@ cudaError_t launch_plain_record(const dsmc_params &p, const DevTables &t, long l
                                 long long n, const RecordArgs &ra, int *filled, int num_sms,
                                 cudaStream_t stream);
 
+// Fed-state pushes (n particles, up to nsteps steps each; pos/vel [n][3] in place).
+cudaError_t launch_push_fp64(const dsmc_params &p, long long n, int nsteps, double *pos,
+                             double *vel, int *status, int *taken, cudaStream_t stream);
+cudaError_t launch_push_fp32(const dsmc_params &p, long long n, int nsteps, double *pos,
+                             double *vel, int *status, int *taken, cudaStream_t stream);
+
+// FMA-throughput probe (kernel_peak.cu); scratch holds `blocks` elements.
+cudaError_t launch_fma_peak(bool fp64, void *scratch, int blocks, int iters, cudaStream_t stream);
+
 // Per-cell FP64 CDF fits (kernel_fit.cu).
 cudaError_t launch_fit_samples(int ncell, int max_per_cell, const double *speeds,
                                const int *counts, int degree, double *coef, double *box,

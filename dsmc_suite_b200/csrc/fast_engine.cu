@@ -1,13 +1,1083 @@
-// fast_engine.cu - resident-slot engine (placeholder until the FP32 path lands).
+// fast_engine.cu - the FAST_FP32 path: resident particle slots, a device work queue, an FP32
+// push with two-sum compensated position and velocity, cell tracking by comparisons, and
+// register run-length deposits flushed as 64-bit fixed-point atomics.
+//
+// Per step the hot loop does one gravity evaluation (one rsqrt), the reference's Verlet variant
+// (src/common/integrator.c:21-44) with the position and velocity sums kept as (hi, lo) float
+// pairs, shell/latitude/longitude tracking against precomputed boundary tables (no asin, atan2
+// or log), photolysis as W0 * 2^(-c * n_day) (one ex2), and a deposit into the register run.
+// Rare events (launch, landing, collision, end of life) leave the loop for code that works in
+// FP32 with FP64 where the reference's classification needs it (launch energy).
 #include "fast_engine.h"
+#include "dsmc_kernels.h"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
 
 namespace dsmc {
+namespace {
 
-FastEngine::~FastEngine() = default;
+constexpr float kPiF = 3.14159265358979f;
 
-cudaError_t FastEngine::run(const dsmc_params &, const DevTables &, bool, long long, long long,
-                            int, cudaStream_t) {
-    return cudaErrorNotSupported;
+__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
+    s = a + b;
+    const float bp = s - a;
+    e = (a - (s - bp)) + (b - bp);
+}
+
+// u in (0, 1): 24 random bits plus half an ulp, so 1 - u and u are never 0.
+__device__ __forceinline__ float unit_open(uint32_t w) {
+    return (static_cast<float>(w >> 8) + 0.5f) * (1.0f / 16777216.0f);
+}
+
+struct FastArgs {
+    const FastInst *inst;
+    int ninst;
+    Slots s;
+    long long nslots;
+    FastCounters *ctr;
+    long long total;
+    int K;
+};
+
+// Per-thread working copy of one slot.
+struct Reg {
+    int inst;
+    unsigned pid, evt;
+    float sh[3], sl[3], vh[3], vl[3], oa[3];
+    float w0;
+    int nday, steps, hop, cell, run_cell;
+    unsigned long long run_acc;
+    int hist_key, hist_cnt;
+    float pcol, pthr;
+    int ncol;
+    float rest, thi0;
+};
+
+__device__ __forceinline__ void load_slot(const Slots &s, long long i, long long S, Reg &r) {
+    r.inst = s.inst[i];
+    r.pid = s.pid[i];
+    r.evt = s.evt[i];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        r.sh[k] = s.sh[k * S + i];
+        r.sl[k] = s.sl[k * S + i];
+        r.vh[k] = s.vh[k * S + i];
+        r.vl[k] = s.vl[k * S + i];
+        r.oa[k] = s.oa[k * S + i];
+    }
+    r.w0 = s.w0[i];
+    r.nday = s.nday[i];
+    r.steps = s.steps[i];
+    r.hop = s.hop[i];
+    r.cell = s.cell[i];
+    r.run_cell = s.run_cell[i];
+    r.run_acc = s.run_acc[i];
+    r.hist_key = s.hist_key[i];
+    r.hist_cnt = s.hist_cnt[i];
+    r.pcol = s.pcol[i];
+    r.pthr = s.pthr[i];
+    r.ncol = s.ncol[i];
+    r.rest = s.rest[i];
+    r.thi0 = s.thi0[i];
+}
+
+__device__ __forceinline__ void store_slot(const Slots &s, long long i, long long S, const Reg &r) {
+    s.inst[i] = r.inst;
+    s.pid[i] = r.pid;
+    s.evt[i] = r.evt;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        s.sh[k * S + i] = r.sh[k];
+        s.sl[k * S + i] = r.sl[k];
+        s.vh[k * S + i] = r.vh[k];
+        s.vl[k * S + i] = r.vl[k];
+        s.oa[k * S + i] = r.oa[k];
+    }
+    s.w0[i] = r.w0;
+    s.nday[i] = r.nday;
+    s.steps[i] = r.steps;
+    s.hop[i] = r.hop;
+    s.cell[i] = r.cell;
+    s.run_cell[i] = r.run_cell;
+    s.run_acc[i] = r.run_acc;
+    s.hist_key[i] = r.hist_key;
+    s.hist_cnt[i] = r.hist_cnt;
+    s.pcol[i] = r.pcol;
+    s.pthr[i] = r.pthr;
+    s.ncol[i] = r.ncol;
+    s.rest[i] = r.rest;
+    s.thi0[i] = r.thi0;
+}
+
+__device__ __forceinline__ void set_pos(Reg &r, const double s[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        r.sh[k] = static_cast<float>(s[k]);
+        r.sl[k] = static_cast<float>(s[k] - static_cast<double>(r.sh[k]));
+    }
+}
+
+__device__ __forceinline__ void set_vel(Reg &r, const double v[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        r.vh[k] = static_cast<float>(v[k]);
+        r.vl[k] = static_cast<float>(v[k] - static_cast<double>(r.vh[k]));
+    }
+}
+
+__device__ __forceinline__ void get_pos(const Reg &r, double s[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) s[k] = static_cast<double>(r.sh[k]) + static_cast<double>(r.sl[k]);
+}
+
+__device__ __forceinline__ void get_vel(const Reg &r, double v[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[k] = static_cast<double>(r.vh[k]) + static_cast<double>(r.vl[k]);
+}
+
+__device__ __forceinline__ int pack_cell(int ht, int td, int fd) { return (ht << 16) | (td << 8) | fd; }
+
+// Latitude row and longitude column of position (x, y, z) with r2 = |s|^2, moved from the
+// current (td, fd) by boundary comparisons. Row td covers latitudes (b_td, b_td+1] and column fd
+// longitudes (phi_fd, phi_fd+1], the upper-inclusive cells of grid_spherical_to_index
+// (src/common/grid.c:28-39).
+__device__ __forceinline__ void track_angles(const FastInst &I, float x, float y, float z, float r2,
+                                             int &td, int &fd) {
+    const int ftd = I.p.ftd, ffd = I.p.ffd;
+    const float zz = z * fabsf(z);
+    for (int it = 0; it < 64 && td + 1 < ftd && zz > r2 * __ldg(I.sbs + td + 1); it++) td++;
+    for (int it = 0; it < 64 && td > 0 && zz <= r2 * __ldg(I.sbs + td); it++) td--;
+    for (int it = 0; it < 2 * 256; it++) {
+        const float2 hi = __ldg(I.lonb + fd + 1);
+        if (x * hi.y - y * hi.x > 0.0f) { fd = fd + 1 == ffd ? 0 : fd + 1; continue; }
+        const float2 lo = __ldg(I.lonb + fd);
+        if (x * lo.y - y * lo.x <= 0.0f && !(fd == 0 && x >= 0.0f && y > 0.0f)) {
+            fd = fd == 0 ? ffd - 1 : fd - 1;
+            continue;
+        }
+        break;
+    }
+}
+
+__device__ __forceinline__ void track_shell(const FastInst &I, float r2, int &ht) {
+    const int hd = I.p.hd;
+    for (int it = 0; it < 64 && ht + 1 < hd && r2 > __ldg(I.rb2 + ht + 1); it++) ht++;
+    for (int it = 0; it < 64 && ht > 0 && r2 <= __ldg(I.rb2 + ht); it++) ht--;
+}
+
+// Cell of a position from scratch: an estimate from the angles, then the comparison fix-up.
+__device__ void cell_from_scratch(const FastInst &I, const float x, const float y, const float z,
+                                  int &ht, int &td, int &fd) {
+    const float r2 = x * x + y * y + z * z;
+    const float r = sqrtf(r2);
+    float th = asinf(fminf(1.0f, fmaxf(-1.0f, z / r)));
+    float ph = atan2f(x, y);
+    if (ph < 0.0f) ph += 2.0f * kPiF;
+    td = static_cast<int>((th + 0.5f * kPiF) / kPiF * I.p.ftd);
+    fd = static_cast<int>(ph / (2.0f * kPiF) * I.p.ffd);
+    td = min(max(td, 0), I.p.ftd - 1);
+    fd = min(max(fd, 0), I.p.ffd - 1);
+    track_angles(I, x, y, z, r2, td, fd);
+    ht = 0;
+    if (I.p.use_exp_grid) {
+        const double arg = I.p.alpha2 * (static_cast<double>(r) - I.p.Radii) / I.p.unih + 1.0;
+        ht = arg <= 1.0 ? 0 : static_cast<int>(log(arg) / I.p.log1p_alpha2);
+    } else {
+        ht = static_cast<int>((static_cast<double>(r) - I.p.Radii) / I.p.unih);
+    }
+    ht = min(max(ht, 0), I.p.hd - 1);
+    track_shell(I, r2, ht);
+}
+
+__device__ __forceinline__ double cdf_eval(const double *coef, const double *box, int degree,
+                                           double x) {
+    const double t = (x - box[2]) / box[3];
+    double r = 0.0;
+    for (int i = 0; i <= degree; i++) r = r * t + coef[i];
+    return r;
+}
+
+// Bisection of the fitted reverse-cumulative speed distribution (collision.c:43-101).
+__device__ double cdf_sample(const double *coef, const double *box, double total, int degree,
+                             double u) {
+    const double at_max = cdf_eval(coef, box, degree, box[1]);
+    const double ranking = u * (total - at_max) + at_max;
+    double v0 = box[0], v1 = box[1];
+    for (int iter = 0; iter < 100; iter++) {
+        const double vm = (v0 + v1) * 0.5;
+        const double fm = cdf_eval(coef, box, degree, vm) - ranking;
+        const double f1 = cdf_eval(coef, box, degree, v1) - ranking;
+        if (fm * f1 < 0) v0 = vm;
+        else v1 = vm;
+        if (fabs(v1 - v0) < 0.01) break;
+    }
+    return (v0 + v1) * 0.5;
+}
+
+__device__ __forceinline__ void unit_sphere_f(float zu, float pu, float o[3]) {
+    const float z = 2.0f * zu - 1.0f;
+    const float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    float sn, cs;
+    sincosf(2.0f * kPiF * pu, &sn, &cs);
+    o[0] = rr * cs;
+    o[1] = rr * sn;
+    o[2] = z;
+}
+
+struct StatAcc {
+    unsigned steps = 0, escaped = 0, collisions = 0, bound = 0, finished = 0;
+    int inst = -1;
+};
+
+// Adds the thread's statistics into its instance's counters: lanes of one instance are summed
+// with one warp reduction and one atomic per counter. Every lane of the warp must call it.
+__device__ void flush_stats(const FastArgs &a, StatAcc &st) {
+    const unsigned full = 0xffffffffu;
+    const int key = st.inst;
+    const unsigned group = __match_any_sync(full, key);
+    const unsigned v[5] = {st.steps, st.escaped, st.collisions, st.bound, st.finished};
+    const int slot_of[5] = {kStatSteps, kStatEscaped, kStatCollisions, kStatBound, kStatFinished};
+    const bool leader = (threadIdx.x & 31) == (__ffs(group) - 1);
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const unsigned sum = __reduce_add_sync(group, v[k]);
+        if (leader && key >= 0 && sum) atomicAdd(&a.inst[key].t.stats[slot_of[k]], static_cast<unsigned long long>(sum));
+    }
+    st = StatAcc{};
+}
+
+__device__ __forceinline__ void flush_run(const FastInst &I, Reg &r) {
+    if (r.run_cell >= 0 && r.run_acc) atomicAdd(&I.t.density[r.run_cell], r.run_acc);
+    r.run_cell = -1;
+    r.run_acc = 0;
+    if (r.hist_key >= 0 && r.hist_cnt) atomicAdd(&I.t.speed_hist[r.hist_key], static_cast<unsigned long long>(r.hist_cnt));
+    r.hist_key = -1;
+    r.hist_cnt = 0;
+}
+
+__device__ __forceinline__ float weight(const FastInst &I, const Reg &r) {
+    return r.w0 * exp2f(-I.c_day * static_cast<float>(r.nday));
+}
+
+// Launch from the current surface position. Returns false when the reference's launch-speed
+// escape test fires (the particle ends as escaped).
+__device__ bool launch(const FastInst &I, Reg &r, StatAcc &st, float local_T, float thi, float fi) {
+    const dsmc_params &p = I.p;
+    Philox rng;
+    rng.init(p.seed, p.instance, r.pid);
+    rng.event = r.evt;
+    rng.next();
+    r.evt = rng.event;
+    double s[3];
+    get_pos(r, s);
+    float v[3];
+    if (p.model == DSMC_MODEL_REFERENCE) {
+        // ballistic.c:125,156-173 in FP32
+        const float KF = 2.0f * kPiF * static_cast<float>(p.Radii) * fabsf(cosf(thi)) / static_cast<float>(p.P);
+        int idx = local_T >= 220.0f ? 20 : static_cast<int>(ceilf(local_T / 10.0f)) - 2;
+        idx = idx < 0 ? 0 : (idx >= 23 ? 22 : idx);
+        const float vr = static_cast<float>(I.t.vt_speeds[idx * 1000 + rng.w[0] % static_cast<uint32_t>(I.t.vt_count[idx])]);
+        float vold2 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3; k++) vold2 += r.vh[k] * r.vh[k];
+        const float alpha = static_cast<float>(p.alpha);
+        const float vout = sqrtf(alpha * vr * vr + (1.0f - alpha) * vold2);
+        const float flyd = static_cast<float>(rng.w[1]) * (kPiF / 4294967296.0f) + thi - 0.5f * kPiF;
+        const float xi = static_cast<float>(rng.w[2]) * (kPiF / 4294967296.0f) + fi - 0.5f * kPiF;
+        float sf, cf, sx, cx, sr, cr;
+        sincosf(flyd, &sf, &cf);
+        sincosf(xi, &sx, &cx);
+        sincosf(fi + 0.5f * kPiF, &sr, &cr);
+        v[0] = cf * sx * vout + KF * sr;
+        v[1] = cf * cx * vout + KF * cr;
+        v[2] = sf * vout;
+        if (sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) >= static_cast<float>(p.ve)) return false;
+    } else {
+        // flux-weighted Maxwell-Boltzmann: Rayleigh normal and Gaussian tangential components
+        // the same maps of the random words as the FP64 path: log(1 - u) and angle 2 pi u
+        const float sigma = sqrtf(static_cast<float>(p.kB_over_m) * local_T);
+        const float vn = sigma * sqrtf(-2.0f * logf(1.0f - unit_open(rng.w[0])));
+        const float rho = sqrtf(-2.0f * logf(1.0f - unit_open(rng.w[1])));
+        float sa, ca;
+        sincosf(2.0f * kPiF * unit_open(rng.w[2]), &sa, &ca);
+        const float t1 = rho * ca, t2 = rho * sa;
+        const float R = sqrtf(static_cast<float>(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]));
+        const float n[3] = {static_cast<float>(s[0]) / R, static_cast<float>(s[1]) / R, static_cast<float>(s[2]) / R};
+        float e[3] = {-n[1], n[0], 0.0f};
+        const float le = sqrtf(e[0] * e[0] + e[1] * e[1]);
+        if (le < 1e-6f) { e[0] = 1.0f; e[1] = 0.0f; }
+        else { e[0] /= le; e[1] /= le; }
+        const float nt[3] = {n[1] * e[2] - n[2] * e[1], n[2] * e[0] - n[0] * e[2], n[0] * e[1] - n[1] * e[0]};
+        const float omega = p.P > 0.0 ? static_cast<float>(2.0 * kPi / p.P) : 0.0f;
+        const float rot[3] = {omega * static_cast<float>(s[1]), -omega * static_cast<float>(s[0]), 0.0f};
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = vn * n[k] + (sigma * t1) * e[k] + (sigma * t2) * nt[k] + rot[k];
+        // FP64 escape/bound classification of the launch
+        const double v2 = static_cast<double>(v[0]) * v[0] + static_cast<double>(v[1]) * v[1] +
+                          static_cast<double>(v[2]) * v[2];
+        const double E = 0.5 * v2 - p.GM / sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+        if (E < 0.0) st.bound++;
+    }
+    const double vd[3] = {v[0], v[1], v[2]};
+    set_vel(r, vd);
+    const double R0 = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    const double g = p.GM / (R0 * R0 * R0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) r.oa[k] = static_cast<float>(g * s[k]);
+    r.hop = 0;
+    return true;
+}
+
+
+__device__ __forceinline__ void ref_index(float thi, float fi, int ftd, int ffd, int &td, int &fd) {
+    td = static_cast<int>(ceilf((thi + 0.5f * kPiF) / kPiF * ftd)) - 1;
+    fd = static_cast<int>(ceilf(fi / (2.0f * kPiF) * ffd)) - 1;
+    td = min(max(td, 0), ftd - 1);
+    fd = min(max(fd, 0), ffd - 1);
+}
+
+__device__ __forceinline__ void angles_of(const Reg &r, float &thi, float &fi) {
+    double s[3];
+    get_pos(r, s);
+    const double R = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    thi = static_cast<float>(asin(s[2] / R));
+    double f = atan2(s[0], s[1]);
+    if (f < 0) f += 2.0 * kPi;
+    fi = static_cast<float>(f);
+}
+
+__device__ __forceinline__ void horizon_add(const FastInst &I, int td, int fd, float W) {
+    atomicAdd(&I.t.horizon[td * I.p.ffd + fd], __float2ull_rn(W * 16777216.0f));
+}
+
+// Start of a hop (ballistic.c:124-181, advanced.c:271-333): weight and life checks, the
+// reference freeze scan, the launch and the starting cell. Returns 0 when the particle flies,
+// else its fate.
+__device__ int hop_top(const FastInst &I, Reg &r, StatAcc &st, float &thi, float &fi,
+                       float local_T) {
+    const dsmc_params &p = I.p;
+    const float W = weight(I, r);
+    if (W < static_cast<float>(p.w_min)) return DSMC_FATE_PHOTOLYSED;
+    if (p.life_step_cap > 0 && r.steps >= p.life_step_cap) return DSMC_FATE_STEP_CAP;
+    if (p.model == DSMC_MODEL_REFERENCE) {
+        const int ftd = p.ftd, ffd = p.ffd;
+        int td, fd;
+        ref_index(thi, fi, ftd, ffd, td, fd);
+        const double *T = I.t.T_map;
+        local_T = static_cast<float>(T[td * ffd + fd]);
+        if (local_T < static_cast<float>(p.freeze_T)) {
+            bool found = false;
+            if (p.runner == DSMC_RUNNER_BALLISTIC) {
+                for (int add = 0; add < ffd; add++) {
+                    r.rest += static_cast<float>(p.dt_rot);
+                    const int check = (fd + add + 1) % ffd;
+                    if (T[td * ffd + check] >= p.freeze_T) {
+                        fd = check;
+                        fi = (fd + 0.5f) / ffd * 2.0f * kPiF;
+                        found = true;
+                        break;
+                    }
+                }
+            } else {
+                horizon_add(I, td, fd, W);
+                for (int add = 1; add <= ffd; add++) {
+                    r.rest += static_cast<float>(p.dt_rot);
+                    if (T[td * ffd + (add % ffd)] >= p.freeze_T) {
+                        const double rot_fi = static_cast<double>(add - fd) / ffd * 2.0 * kPi;
+                        const double cs = cos(rot_fi), sn = sin(rot_fi);
+                        double s[3];
+                        get_pos(r, s);
+                        const double n0 = s[0] * cs - s[1] * sn, n1 = s[0] * sn + s[1] * cs;
+                        s[0] = n0;
+                        s[1] = n1;
+                        set_pos(r, s);
+                        fd = add % ffd;
+                        fi = (fd + 0.5f) / ffd * 2.0f * kPiF;
+                        found = true;
+                        break;
+                    }
+                }
+            }
+            if (!found) {
+                horizon_add(I, td, fd, W);
+                return DSMC_FATE_FROZEN;
+            }
+            local_T = static_cast<float>(T[td * ffd + fd]);
+        }
+    }
+    if (!launch(I, r, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
+    int ht, td, fd;
+    cell_from_scratch(I, r.sh[0] + r.sl[0], r.sh[1] + r.sl[1], r.sh[2] + r.sl[2], ht, td, fd);
+    r.cell = pack_cell(ht, td, fd);
+    return 0;
+}
+
+// Landing (ballistic.c:239-264): polar deposit (reference) or night freeze-out / day-side
+// re-emission point (config). Returns 0 to start a new hop, else the fate.
+__device__ int land(const FastInst &I, Reg &r, float &thi, float &fi, float &local_T) {
+    const dsmc_params &p = I.p;
+    angles_of(r, thi, fi);
+    int td, fd;
+    ref_index(thi, fi, p.ftd, p.ffd, td, fd);
+    if (p.model == DSMC_MODEL_REFERENCE) {
+        if (td <= 1 || td >= p.ftd - 2) {
+            horizon_add(I, td, fd, 0.05f * weight(I, r));
+            r.w0 *= 0.95f;
+        }
+        return 0;
+    }
+    double s[3];
+    get_pos(r, s);
+    const double R = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    double n[3] = {s[0] / R, s[1] / R, s[2] / R};
+    if (n[0] * p.sun[0] + n[1] * p.sun[1] + n[2] * p.sun[2] <= 0.0) {
+        horizon_add(I, td, fd, weight(I, r));
+        return DSMC_FATE_FROZEN;
+    }
+    for (int k = 0; k < 3; k++) s[k] = n[k] * p.Radii;
+    set_pos(r, s);
+    local_T = static_cast<float>(I.t.face_T[locate_face(I.t, n)]);
+    return 0;
+}
+
+// End of a particle's life: per-particle rows, counters, deposit runs flushed.
+__device__ void finish(const FastInst &I, Reg &r, StatAcc &st, int fate) {
+    const dsmc_params &p = I.p;
+    const DevTables &t = I.t;
+    const bool ref = p.model == DSMC_MODEL_REFERENCE, adv = p.runner == DSMC_RUNNER_ADVANCED;
+    const long long slot = static_cast<long long>(r.pid) - t.out_base;
+    if (slot >= 0 && slot < t.out_cap) {
+        if (t.ttime && (fate != DSMC_FATE_ESCAPED || !ref)) {
+            float thi, fi;
+            angles_of(r, thi, fi);
+            const double flight = static_cast<double>(r.steps) * p.dt_step;
+            t.ttime[1 * t.out_cap + slot] = thi;
+            t.ttime[2 * t.out_cap + slot] = flight + r.rest;
+            t.ttime[3 * t.out_cap + slot] = weight(I, r);
+            t.ttime[4 * t.out_cap + slot] = flight;
+            if (adv || !ref) {
+                t.ttime[7 * t.out_cap + slot] = r.rest;
+                t.ttime[8 * t.out_cap + slot] = r.ncol;
+            }
+        }
+        if (t.fate) t.fate[slot] = fate;
+        if (t.steps) t.steps[slot] = r.steps;
+    }
+    st.finished++;
+    st.collisions += r.ncol;
+    if (fate == DSMC_FATE_ESCAPED) st.escaped++;
+    flush_run(I, r);
+    r.inst = -1;
+}
+
+// A collision against a partner drawn from the cell's fitted speed CDF (advanced.c:374-396).
+__device__ void collide(const FastInst &I, Reg &r, long long pidx) {
+    const dsmc_params &p = I.p;
+    const DevTables &t = I.t;
+    Philox rng;
+    rng.init(p.seed, p.instance, r.pid);
+    rng.event = r.evt;
+    rng.next();
+    const double *coef = t.cdf_coef + DSMC_CDF_STRIDE * pidx;
+    const double *box = t.cdf_box + 4 * pidx;
+    double v[3];
+    get_vel(r, v);
+    const double vv2 = cdf_sample(coef, box, t.cdf_total[pidx], t.cdf_degree, rng.raw(0) / kTwo32);
+    double col_p = -1.0;
+    if (p.scatter == DSMC_SCATTER_REFERENCE) {
+        const double thi2 = kPi * rng.raw(1) / kTwo32 - kPi / 2.0;
+        const double fi2 = 2.0 * kPi * rng.raw(2) / kTwo32;
+        const double v2[3] = {vv2 * cos(thi2) * cos(fi2), vv2 * cos(thi2) * sin(fi2), vv2 * sin(thi2)};
+        for (int k = 0; k < 3; k++) v[k] = (v[k] + v2[k]) + 0.5 * (v[k] - v2[k]);
+        if (p.redraw_col_threshold) col_p = rng.raw(3) / kTwo32;
+    } else {
+        float d2[3], om[3];
+        unit_sphere_f(unit_open(rng.w[1]), unit_open(rng.w[2]), d2);
+        if (p.redraw_col_threshold) col_p = rng.raw(3) / kTwo32;
+        rng.next();
+        unit_sphere_f(unit_open(rng.w[0]), unit_open(rng.w[1]), om);
+        double g2 = 0.0, vcm[3];
+        for (int k = 0; k < 3; k++) {
+            const double v2k = vv2 * d2[k];
+            g2 += (v[k] - v2k) * (v[k] - v2k);
+            vcm[k] = 0.5 * (v[k] + v2k);
+        }
+        const double hg = 0.5 * sqrt(g2);
+        for (int k = 0; k < 3; k++) v[k] = vcm[k] + hg * om[k];
+    }
+    r.evt = rng.event;
+    if (col_p >= 0.0) r.pthr = static_cast<float>(-log1p(-col_p));
+    set_vel(r, v);
+    r.pcol = 0.0f;
+    r.ncol++;
+}
+
+// Next work index of the device queue: one atomic per group of lanes asking together.
+__device__ __forceinline__ unsigned long long grab_work(FastCounters *ctr) {
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    const unsigned rank = __popc(m & ((1u << lane) - 1u));
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(&ctr->next, static_cast<unsigned long long>(__popc(m)));
+    base = __shfl_sync(m, base, leader);
+    return base + rank;
+}
+
+__device__ __forceinline__ int find_inst(const FastArgs &a, unsigned long long w) {
+    int lo = 0, hi = a.ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (static_cast<unsigned long long>(a.inst[mid].work_base) <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Fill an empty slot with the next particle from the queue and launch it; particles that end
+// at their first launch are finished here and the next one is taken. Returns false when the
+// queue is empty.
+__device__ bool start_next(const FastArgs &a, Reg &r, StatAcc &st) {
+    for (;;) {
+        const unsigned long long w = grab_work(a.ctr);
+        if (w >= static_cast<unsigned long long>(a.total)) return false;
+        const int ii = find_inst(a, w);
+        const FastInst &I = a.inst[ii];
+        const dsmc_params &p = I.p;
+        if (ii != st.inst) {
+            // counters belong to one instance: add the previous instance's share lane by lane
+            if (st.inst >= 0) {
+                unsigned long long *dst = a.inst[st.inst].t.stats;
+                if (st.steps) atomicAdd(dst + kStatSteps, static_cast<unsigned long long>(st.steps));
+                if (st.escaped) atomicAdd(dst + kStatEscaped, static_cast<unsigned long long>(st.escaped));
+                if (st.collisions) atomicAdd(dst + kStatCollisions, static_cast<unsigned long long>(st.collisions));
+                if (st.bound) atomicAdd(dst + kStatBound, static_cast<unsigned long long>(st.bound));
+                if (st.finished) atomicAdd(dst + kStatFinished, static_cast<unsigned long long>(st.finished));
+                if (st.finished) atomicAdd(&a.ctr->finished, static_cast<unsigned long long>(st.finished));
+            }
+            st = StatAcc{};
+            st.inst = ii;
+        }
+        r.inst = ii;
+        r.pid = static_cast<unsigned>(I.pid_begin + static_cast<long long>(w - I.work_base));
+        Philox rng;
+        rng.init(p.seed, p.instance, r.pid);
+        rng.next();
+        r.w0 = 1.0f;
+        r.nday = 0;
+        r.steps = 0;
+        r.hop = 0;
+        r.pcol = 0.0f;
+        r.ncol = 0;
+        r.rest = 0.0f;
+        r.run_cell = -1;
+        r.run_acc = 0;
+        r.hist_key = -1;
+        r.hist_cnt = 0;
+        const double zero[3] = {0.0, 0.0, 0.0};
+        set_vel(r, zero);
+        float thi, fi, local_T = 0.0f;
+        double col_p = 0.0;
+        double s[3];
+        if (p.model == DSMC_MODEL_REFERENCE) {
+            const bool adv = p.runner == DSMC_RUNNER_ADVANCED;
+            if (adv) col_p = rng.raw(0) / kTwo32;
+            const int o = adv ? 1 : 0;
+            const double th = rng.raw(o) / kTwo32 * kPi - kPi / 2.0;
+            const double ph = rng.raw(o + 1) / kTwo32 * 2.0 * kPi;
+            s[0] = p.Radii * cos(th) * sin(ph);
+            s[1] = p.Radii * cos(th) * cos(ph);
+            s[2] = p.Radii * sin(th);
+            thi = static_cast<float>(th);
+            fi = static_cast<float>(ph);
+            int td, fd;
+            ref_index(thi, fi, p.ftd, p.ffd, td, fd);
+            local_T = static_cast<float>(I.t.T_map[td * p.ffd + fd]);
+        } else {
+            const int f = pick_face(I.t, rng.raw(0) / kTwo32);
+            double u1 = rng.raw(1) / kTwo32, u2 = rng.raw(2) / kTwo32;
+            col_p = rng.raw(3) / kTwo32;
+            if (u1 + u2 > 1.0) { u1 = 1.0 - u1; u2 = 1.0 - u2; }
+            const double *fv = I.t.face_verts + 9 * f;
+            double q[3];
+            for (int k = 0; k < 3; k++) q[k] = fv[k] + u1 * (fv[3 + k] - fv[k]) + u2 * (fv[6 + k] - fv[k]);
+            const double lq = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+            for (int k = 0; k < 3; k++) s[k] = q[k] * (p.Radii / lq);
+            local_T = static_cast<float>(I.t.face_T[f]);
+        }
+        r.evt = rng.event;
+        r.pthr = static_cast<float>(-log1p(-col_p));
+        set_pos(r, s);
+        if (p.model != DSMC_MODEL_REFERENCE) angles_of(r, thi, fi);
+        r.thi0 = thi;
+        const long long slot = static_cast<long long>(r.pid) - I.t.out_base;
+        if (I.t.ttime && slot >= 0 && slot < I.t.out_cap) {
+            I.t.ttime[slot] = thi;
+            if (p.runner == DSMC_RUNNER_ADVANCED || p.model != DSMC_MODEL_REFERENCE) {
+                I.t.ttime[5 * I.t.out_cap + slot] = fi;
+                I.t.ttime[6 * I.t.out_cap + slot] = local_T;
+            }
+        }
+        const int fate = hop_top(I, r, st, thi, fi, local_T);
+        if (fate == 0) return true;
+        finish(I, r, st, fate);
+    }
+}
+
+// One Verlet step of the reference's variant with (hi, lo) position and velocity sums.
+// (x, y, z, r2) hold the current position on entry and the new one on exit; d the displacement.
+__device__ __forceinline__ void verlet_f32(Reg &r, float &x, float &y, float &z, float &r2,
+                                           float GM, float h, float c1, float c2, float d[3]) {
+    const float ir = rsqrtf(r2);
+    const float g = GM * (ir * ir * ir);
+    const float a[3] = {g * x, g * y, g * z};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        d[k] = fmaf(r.vh[k], h, fmaf(r.vl[k], h, -fmaf(a[k], c1, r.oa[k] * c2)));
+        float t, e;
+        two_sum(r.sh[k], d[k], t, e);
+        r.sh[k] = t;
+        r.sl[k] += e;
+        two_sum(r.vh[k], -a[k] * h, t, e);
+        r.vh[k] = t;
+        r.vl[k] += e;
+        r.oa[k] = a[k];
+    }
+    x = r.sh[0] + r.sl[0];
+    y = r.sh[1] + r.sl[1];
+    z = r.sh[2] + r.sl[2];
+    r2 = fmaf(x, x, fmaf(y, y, z * z));
+}
+
+__global__ void __launch_bounds__(256, 2) fast_kernel(const FastArgs a) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    Reg r;
+    load_slot(a.s, i, a.nslots, r);
+    StatAcc st;
+    st.inst = r.inst;
+    int budget = a.K;
+    bool alive = r.inst >= 0;
+    if (!alive) alive = start_next(a, r, st);
+    // constants of the current particle's instance
+    int cur = -1;
+    float GM = 0.f, h = 0.f, c1 = 0.f, c2 = 0.f, rl2 = 0.f, re2 = 0.f, cday = 0.f, sun0 = 0.f,
+          sun1 = 0.f, sun2 = 0.f, sig = 0.f, inv_bw = 0.f, wmin = 0.f;
+    int ftd = 0, ffd = 0, hd = 0, nbins = 0, col_ht = 0;
+    bool ref = false, skip_first = false, collide_on = false, hist_on = false;
+    long long life_cap = 0, hop_cap = 0;
+    const FastInst *I = nullptr;
+    float x = 0.f, y = 0.f, z = 0.f, r2 = 0.f;
+    bool fresh = true;
+
+    while (alive && budget > 0) {
+        if (r.inst != cur) {
+            cur = r.inst;
+            I = &a.inst[cur];
+            const dsmc_params &p = I->p;
+            GM = static_cast<float>(p.GM);
+            h = static_cast<float>(p.dt_step);
+            c1 = static_cast<float>(1.5 * p.dt_step * p.dt_step);
+            c2 = static_cast<float>(p.dt_step * p.dt_step / 6.0);
+            rl2 = I->r_land2;
+            re2 = I->r_esc2;
+            cday = I->c_day;
+            sun0 = static_cast<float>(p.sun[0]);
+            sun1 = static_cast<float>(p.sun[1]);
+            sun2 = static_cast<float>(p.sun[2]);
+            ftd = p.ftd; ffd = p.ffd; hd = p.hd;
+            ref = p.model == DSMC_MODEL_REFERENCE;
+            skip_first = p.skip_first_deposit != 0;
+            collide_on = p.runner == DSMC_RUNNER_ADVANCED && I->t.n_bg != nullptr;
+            col_ht = p.collide_ht_max;
+            sig = static_cast<float>(p.cross_section);
+            hist_on = I->t.speed_hist != nullptr && p.n_speed_bins > 0;
+            nbins = p.n_speed_bins;
+            inv_bw = hist_on ? static_cast<float>(1.0 / p.speed_bin_width) : 0.f;
+            life_cap = p.life_step_cap;
+            hop_cap = p.hop_step_cap;
+            wmin = static_cast<float>(p.w_min);
+        }
+        if (fresh) {
+            x = r.sh[0] + r.sl[0];
+            y = r.sh[1] + r.sl[1];
+            z = r.sh[2] + r.sl[2];
+            r2 = fmaf(x, x, fmaf(y, y, z * z));
+            fresh = false;
+        }
+        float d[3];
+        verlet_f32(r, x, y, z, r2, GM, h, c1, c2, d);
+        budget--;
+        const int ii = r.hop;
+        r.steps++;
+        r.hop++;
+        int event = 0;   // 1 landed (or hop cap), 2 escaped, 3 life cap
+        if (r2 <= rl2) {
+            event = 1;
+        } else if (r2 >= re2) {
+            event = 2;
+        } else {
+            int ht = r.cell >> 16, td = (r.cell >> 8) & 0xff, fd = r.cell & 0xff;
+            track_shell(*I, r2, ht);
+            track_angles(*I, x, y, z, r2, td, fd);
+            r.cell = pack_cell(ht, td, fd);
+            const bool day = ref ? (fd < ffd / 2) : (fmaf(x, sun0, fmaf(y, sun1, z * sun2)) > 0.0f);
+            if (day) r.nday++;
+            if (!(skip_first && ii == 0)) {
+                const int ci = (ht * ftd + td) * ffd + fd;
+                bool collided = false;
+                if (collide_on && ht < col_ht) {
+                    const float nb = ci < I->t.n_bg_len ? static_cast<float>(__ldg(I->t.n_bg + ci)) : 0.f;
+                    r.pcol += sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) * nb * sig;
+                    if (r.pcol > r.pthr) {
+                        const long long pidx = (static_cast<long long>(td) * ffd + fd) * hd + ht;
+                        if (__ldg(I->t.cdf_valid + pidx)) {
+                            collide(*I, r, pidx);
+                            collided = true;
+                        }
+                    }
+                }
+                if (!collided) {
+                    const float W = r.w0 * exp2f(-cday * static_cast<float>(r.nday));
+                    const unsigned long long q = __float2ull_rn(W * 16777216.0f);
+                    if (ci == r.run_cell) {
+                        r.run_acc += q;
+                    } else {
+                        if (r.run_cell >= 0) atomicAdd(&I->t.density[r.run_cell], r.run_acc);
+                        r.run_cell = ci;
+                        r.run_acc = q;
+                    }
+                    if (hist_on) {
+                        const float sp = sqrtf(fmaf(r.vh[0], r.vh[0], fmaf(r.vh[1], r.vh[1], r.vh[2] * r.vh[2])));
+                        const int b = min(static_cast<int>(sp * inv_bw), nbins - 1);
+                        const int key = ci * nbins + b;
+                        if (key == r.hist_key) {
+                            r.hist_cnt++;
+                        } else {
+                            if (r.hist_key >= 0) atomicAdd(&I->t.speed_hist[r.hist_key], static_cast<unsigned long long>(r.hist_cnt));
+                            r.hist_key = key;
+                            r.hist_cnt = 1;
+                        }
+                    }
+                }
+            }
+            if (life_cap > 0 && r.steps >= life_cap) event = 3;
+            else if (r.hop >= hop_cap) event = 1;
+        }
+        st.steps++;
+        if (event) {
+            fresh = true;
+            int fate = 0;
+            if (event == 2) {
+                fate = DSMC_FATE_ESCAPED;
+            } else if (event == 3) {
+                fate = DSMC_FATE_STEP_CAP;
+            } else {
+                float thi, fi, local_T = 0.f;
+                fate = land(*I, r, thi, fi, local_T);
+                if (fate == 0) fate = hop_top(*I, r, st, thi, fi, local_T);
+            }
+            if (fate) {
+                finish(*I, r, st, fate);
+                alive = start_next(a, r, st);
+            }
+        }
+        (void)wmin;
+    }
+    if (!alive && r.inst >= 0) {
+        // (not reached: a slot without a particle has inst = -1)
+    }
+    store_slot(a.s, i, a.nslots, r);
+    // statistics of this launch, per instance; the finished count also drives the host loop
+    const unsigned fin = st.finished;
+    flush_stats(a, st);
+    const unsigned full = 0xffffffffu;
+    const unsigned wfin = __reduce_add_sync(full, fin);
+    if ((threadIdx.x & 31) == 0 && wfin) atomicAdd(&a.ctr->finished, static_cast<unsigned long long>(wfin));
+}
+
+// Fed-state FP32 push (dsmc_push_host with FAST_FP32).
+__global__ void push_fp32_kernel(const dsmc_params p, long long n, int nsteps, double *pos,
+                                 double *vel, int *status, int *taken) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Reg r;
+    const double s[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    const double v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+    set_pos(r, s);
+    set_vel(r, v);
+    const double R0 = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    const double g0 = p.GM / (R0 * R0 * R0);
+    for (int k = 0; k < 3; k++) r.oa[k] = static_cast<float>(g0 * s[k]);
+    const float GM = static_cast<float>(p.GM), h = static_cast<float>(p.dt_step);
+    const float c1 = static_cast<float>(1.5 * p.dt_step * p.dt_step);
+    const float c2 = static_cast<float>(p.dt_step * p.dt_step / 6.0);
+    const float rl2 = static_cast<float>(p.Radii * p.Radii);
+    const float re2 = static_cast<float>(p.max_height * p.max_height);
+    float x = r.sh[0] + r.sl[0], y = r.sh[1] + r.sl[1], z = r.sh[2] + r.sl[2];
+    float r2 = fmaf(x, x, fmaf(y, y, z * z));
+    int st = 0, k = 0;
+    for (; k < nsteps && st == 0; k++) {
+        float d[3];
+        verlet_f32(r, x, y, z, r2, GM, h, c1, c2, d);
+        st = r2 <= rl2 ? 1 : (r2 >= re2 ? 2 : 0);
+    }
+    double so[3], vo[3];
+    get_pos(r, so);
+    get_vel(r, vo);
+    for (int j = 0; j < 3; j++) { pos[3 * i + j] = so[j]; vel[3 * i + j] = vo[j]; }
+    status[i] = st;
+    taken[i] = k;
+}
+
+}  // namespace
+
+cudaError_t launch_push_fp32(const dsmc_params &p, long long n, int nsteps, double *pos,
+                             double *vel, int *status, int *taken, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    push_fp32_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, stream>>>(p, n, nsteps, pos, vel,
+                                                                                status, taken);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// Host side.
+
+FastEngine::~FastEngine() { free_all(); }
+
+void FastEngine::free_all() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    if (slot_mem_) cudaFree(slot_mem_);
+    slot_mem_ = nullptr;
+    if (d_inst_) cudaFree(d_inst_);
+    d_inst_ = nullptr;
+    if (d_tab_) cudaFree(d_tab_);
+    d_tab_ = nullptr;
+    if (d_ctr_) cudaFree(d_ctr_);
+    d_ctr_ = nullptr;
+    if (h_ctr_) cudaFreeHost(h_ctr_);
+    h_ctr_ = nullptr;
+    nslots_ = 0;
+}
+
+cudaError_t FastEngine::ensure_slots(int num_sms) {
+    // one wave: as many blocks per SM as can be resident together
+    int resident = 0;
+    cudaError_t e0 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fast_kernel, block, 0);
+    if (e0 != cudaSuccess) return e0;
+    if (resident < 1) return cudaErrorInvalidConfiguration;
+    const int per_sm = (blocks_per_sm > resident || blocks_per_sm < 1) ? resident : blocks_per_sm;
+    nslots_want_changed_ = false;
+    const long long want = static_cast<long long>(num_sms) * per_sm * block;
+    if (slot_mem_ && nslots_ == want) return cudaSuccess;
+    if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+    if (slot_mem_) { cudaFree(slot_mem_); slot_mem_ = nullptr; }
+    const long long S = want;
+    // 4-byte fields: inst pid evt (3) + 15 vector floats + w0 nday steps hop cell run_cell
+    // hist_key hist_cnt pcol pthr ncol rest thi0 (13) = 31 words; plus run_acc (8 bytes).
+    const size_t bytes = static_cast<size_t>(S) * (31 * 4 + 8) + 256;
+    cudaError_t e = cudaMalloc(&slot_mem_, bytes);
+    if (e != cudaSuccess) return e;
+    char *b = static_cast<char *>(slot_mem_);
+    auto take = [&](size_t each) { char *p = b; b += static_cast<size_t>(S) * each; return p; };
+    slots_.run_acc = reinterpret_cast<unsigned long long *>(take(8));
+    slots_.inst = reinterpret_cast<int *>(take(4));
+    slots_.pid = reinterpret_cast<unsigned *>(take(4));
+    slots_.evt = reinterpret_cast<unsigned *>(take(4));
+    slots_.sh = reinterpret_cast<float *>(take(12));
+    slots_.sl = reinterpret_cast<float *>(take(12));
+    slots_.vh = reinterpret_cast<float *>(take(12));
+    slots_.vl = reinterpret_cast<float *>(take(12));
+    slots_.oa = reinterpret_cast<float *>(take(12));
+    slots_.w0 = reinterpret_cast<float *>(take(4));
+    slots_.nday = reinterpret_cast<int *>(take(4));
+    slots_.steps = reinterpret_cast<int *>(take(4));
+    slots_.hop = reinterpret_cast<int *>(take(4));
+    slots_.cell = reinterpret_cast<int *>(take(4));
+    slots_.run_cell = reinterpret_cast<int *>(take(4));
+    slots_.hist_key = reinterpret_cast<int *>(take(4));
+    slots_.hist_cnt = reinterpret_cast<int *>(take(4));
+    slots_.pcol = reinterpret_cast<float *>(take(4));
+    slots_.pthr = reinterpret_cast<float *>(take(4));
+    slots_.ncol = reinterpret_cast<int *>(take(4));
+    slots_.rest = reinterpret_cast<float *>(take(4));
+    slots_.thi0 = reinterpret_cast<float *>(take(4));
+    nslots_ = S;
+    if (!d_ctr_) {
+        if ((e = cudaMalloc(&d_ctr_, sizeof(FastCounters))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&h_ctr_, sizeof(FastCounters))) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t FastEngine::upload_instances(const std::vector<dsmc_params> &ps,
+                                         const std::vector<DevTables> &ts,
+                                         const std::vector<long long> &counts,
+                                         const std::vector<long long> &pid_begins,
+                                         cudaStream_t stream) {
+    const int n = static_cast<int>(ps.size());
+    // boundary tables, one block per instance: rb2 [hd+1], sbs [ftd+1], lonb [2*(ffd+1)]
+    std::vector<size_t> off(n);
+    size_t total = 0;
+    for (int k = 0; k < n; k++) {
+        off[k] = total;
+        total += (ps[k].hd + 1) + (ps[k].ftd + 1);
+        total = (total + 1) & ~static_cast<size_t>(1);  // float2 alignment
+        total += 2 * (ps[k].ffd + 1);
+    }
+    std::vector<float> tab(total, 0.0f);
+    std::vector<FastInst> inst(n);
+    long long base = 0;
+    for (int k = 0; k < n; k++) {
+        const dsmc_params &p = ps[k];
+        float *rb2 = tab.data() + off[k];
+        float *sbs = rb2 + (p.hd + 1);
+        size_t lo = off[k] + (p.hd + 1) + (p.ftd + 1);
+        lo = (lo + 1) & ~static_cast<size_t>(1);
+        float *lon = tab.data() + lo;
+        for (int j = 0; j <= p.hd; j++) {
+            const double rj = p.use_exp_grid
+                                  ? p.Radii + p.unih * (std::pow(1.0 + p.alpha2, j) - 1.0) / p.alpha2
+                                  : p.Radii + j * p.unih;
+            rb2[j] = static_cast<float>(rj * rj);
+        }
+        for (int j = 0; j <= p.ftd; j++) {
+            const double b = static_cast<double>(j) / p.ftd * kPi - kPi / 2.0;
+            const double sb = std::sin(b);
+            sbs[j] = static_cast<float>(sb * std::fabs(sb));
+        }
+        sbs[0] = -1.0f;
+        sbs[p.ftd] = 1.0f;
+        for (int j = 0; j <= p.ffd; j++) {
+            const double ph = 2.0 * kPi * j / p.ffd;
+            lon[2 * j] = static_cast<float>(std::sin(ph));
+            lon[2 * j + 1] = static_cast<float>(std::cos(ph));
+        }
+        lon[0] = 0.0f; lon[1] = 1.0f;
+        lon[2 * p.ffd] = 0.0f; lon[2 * p.ffd + 1] = 1.0f;
+        FastInst &I = inst[k];
+        std::memset(&I, 0, sizeof I);
+        I.p = p;
+        I.t = ts[k];
+        I.work_base = base;
+        I.n = counts[k];
+        I.pid_begin = pid_begins[k];
+        I.c_day = static_cast<float>(p.dt_step / p.lifetime / std::log(2.0));
+        I.r_land2 = static_cast<float>(p.Radii * p.Radii);
+        I.r_esc2 = static_cast<float>(p.max_height * p.max_height);
+        // device addresses filled below
+        I.rb2 = reinterpret_cast<const float *>(off[k]);
+        I.sbs = reinterpret_cast<const float *>(off[k] + (p.hd + 1));
+        I.lonb = reinterpret_cast<const float2 *>(lo);
+        base += counts[k];
+    }
+    cudaError_t e;
+    if (total > tab_cap_) {
+        if (d_tab_) cudaFree(d_tab_);
+        d_tab_ = nullptr;
+        if ((e = cudaMalloc(&d_tab_, total * sizeof(float))) != cudaSuccess) return e;
+        tab_cap_ = total;
+        if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+    }
+    if (n > ninst_cap_) {
+        if (d_inst_) cudaFree(d_inst_);
+        d_inst_ = nullptr;
+        if ((e = cudaMalloc(&d_inst_, n * sizeof(FastInst))) != cudaSuccess) return e;
+        ninst_cap_ = n;
+        if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+    }
+    for (auto &I : inst) {
+        I.rb2 = d_tab_ + reinterpret_cast<size_t>(I.rb2);
+        I.sbs = d_tab_ + reinterpret_cast<size_t>(I.sbs);
+        I.lonb = reinterpret_cast<const float2 *>(d_tab_ + reinterpret_cast<size_t>(I.lonb));
+    }
+    if ((e = cudaMemcpyAsync(d_tab_, tab.data(), total * sizeof(float), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(d_inst_, inst.data(), n * sizeof(FastInst), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        return e;
+    ninst_ = n;
+    // the host staging vectors die here: wait for the copies
+    return cudaStreamSynchronize(stream);
+}
+
+cudaError_t FastEngine::drain(long long total, cudaStream_t stream) {
+    cudaError_t e;
+    launches = 0;
+    if (total <= 0) return cudaSuccess;
+    if ((e = cudaMemsetAsync(d_ctr_, 0, sizeof(FastCounters), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(slots_.inst, 0xff, nslots_ * sizeof(int), stream)) != cudaSuccess) return e;
+    FastArgs a{};
+    a.inst = d_inst_;
+    a.ninst = ninst_;
+    a.s = slots_;
+    a.nslots = nslots_;
+    a.ctr = d_ctr_;
+    a.total = total;
+    a.K = steps_per_launch;
+    const unsigned grid = static_cast<unsigned>(nslots_ / block);
+    const int key[4] = {static_cast<int>(total & 0x7fffffff), static_cast<int>(total >> 31), ninst_,
+                        steps_per_launch * 64 + launches_per_graph};
+    const bool use_graph = launches_per_graph > 1;
+    if (use_graph && (!graph_ || graph_stream_ != stream || std::memcmp(key, graph_key_, sizeof key) != 0)) {
+        if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+        cudaGraph_t g;
+        if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+        for (int k = 0; k < launches_per_graph; k++) fast_kernel<<<grid, block, 0, stream>>>(a);
+        if ((e = cudaStreamEndCapture(stream, &g)) != cudaSuccess) return e;
+        e = cudaGraphInstantiate(&graph_, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { graph_ = nullptr; return e; }
+        graph_stream_ = stream;
+        std::memcpy(graph_key_, key, sizeof key);
+    }
+    // Every launch advances each live particle by K steps or ends it, and every life is bounded
+    // by its step caps, so the queue drains. The loop still gives up (launch-timeout status) if
+    // no particle finishes for 4096 rounds, which would mean a logic error, not a long solve.
+    unsigned long long last = 0;
+    long long stalled = 0;
+    for (;;) {
+        if (stalled > 4096) return cudaErrorLaunchTimeout;
+        if (use_graph) {
+            if ((e = cudaGraphLaunch(graph_, stream)) != cudaSuccess) return e;
+            launches += launches_per_graph;
+        } else {
+            fast_kernel<<<grid, block, 0, stream>>>(a);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            launches += 1;
+        }
+        if ((e = cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(FastCounters), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+        if (h_ctr_->finished >= static_cast<unsigned long long>(total)) return cudaSuccess;
+        stalled = h_ctr_->finished == last ? stalled + 1 : 0;
+        last = h_ctr_->finished;
+    }
+}
+
+cudaError_t FastEngine::run(const dsmc_params &p, const DevTables &t, bool fp64, long long pid_begin,
+                            long long n, int num_sms, cudaStream_t stream) {
+    if (fp64) return cudaErrorNotSupported;
+    if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767) return cudaErrorInvalidValue;
+    cudaError_t e = ensure_slots(num_sms);
+    if (e != cudaSuccess) return e;
+    e = upload_instances({p}, {t}, {n}, {pid_begin}, stream);
+    if (e != cudaSuccess) return e;
+    return drain(n, stream);
+}
+
+cudaError_t FastEngine::run_batch(const std::vector<dsmc_params> &ps, const std::vector<DevTables> &ts,
+                                  const std::vector<long long> &counts, int num_sms, cudaStream_t stream) {
+    for (const auto &p : ps)
+        if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767) return cudaErrorInvalidValue;
+    cudaError_t e = ensure_slots(num_sms);
+    if (e != cudaSuccess) return e;
+    std::vector<long long> pid0(ps.size(), 0);
+    e = upload_instances(ps, ts, counts, pid0, stream);
+    if (e != cudaSuccess) return e;
+    long long total = 0;
+    for (long long c : counts) total += c;
+    return drain(total, stream);
 }
 
 }  // namespace dsmc

@@ -1,9 +1,56 @@
 // fast_engine.h - resident-slot engine of the FAST paths (internal to the library).
+//
+// A fixed set of particle slots (one per resident thread) lives in HBM as structure-of-arrays.
+// Each launch advances every slot by up to K Verlet steps; a slot whose particle ends takes the
+// next particle from a device work queue that spans one or many problem instances. The launch
+// loop is captured once as a CUDA graph of G launches and replayed until the queue is drained.
 #pragma once
+
+#include <vector>
 
 #include "dsmc_device.cuh"
 
 namespace dsmc {
+
+// One problem instance as the fast kernel sees it.
+struct FastInst {
+    dsmc_params p;
+    DevTables t;
+    const float *rb2;        // [hd+1] squared shell boundaries, rb2[0] = R^2, rb2[hd] = r_top^2
+    const float *sbs;        // [ftd+1] sin(b)|sin(b)| of latitude boundaries b_k
+    const float2 *lonb;      // [ffd+1] (sin, cos) of longitude boundaries phi_k = 2 pi k / ffd
+    long long work_base;     // first work index of this instance in the queue
+    long long n;             // particles
+    long long pid_begin;     // particle id of the first particle
+    float c_day;             // h / lifetime / ln 2 (W = W0 * 2^(-c_day * n_day))
+    float r_land2, r_esc2;   // Radii^2, max_height^2
+};
+
+// Structure-of-arrays particle slots.
+struct Slots {
+    int *inst;               // instance index, -1 = empty
+    unsigned *pid;           // particle id within its instance
+    unsigned *evt;           // Philox event counter
+    float *sh, *sl, *vh, *vl, *oa;   // [3][S] each: position hi/lo, velocity hi/lo, old accel
+    float *w0;               // weight factor outside photolysis
+    int *nday;               // day-side steps (photolysis exponent)
+    int *steps;              // steps in the particle's life
+    int *hop;                // steps in the current hop
+    int *cell;               // packed (ht << 16) | (td << 8) | fd
+    int *run_cell;           // cell of the register deposit run, -1 = none
+    unsigned long long *run_acc;
+    int *hist_key;           // (cell * nbins + bin) of the speed-histogram run, -1 = none
+    int *hist_cnt;
+    float *pcol, *pthr;      // accumulated collision probability and its threshold
+    int *ncol;
+    float *rest;             // freeze waiting time (reference model)
+    float *thi0;             // launch latitude of the particle (for ttime row 0)
+};
+
+struct FastCounters {
+    unsigned long long next;      // next work index
+    unsigned long long finished;  // particles whose life ended
+};
 
 class FastEngine {
 public:
@@ -12,9 +59,53 @@ public:
     FastEngine(const FastEngine &) = delete;
     FastEngine &operator=(const FastEngine &) = delete;
 
-    // Solve particles [pid_begin, pid_begin + n) to the end of their lives.
+    // Solve particles [pid_begin, pid_begin + n) of one instance to the end of their lives.
     cudaError_t run(const dsmc_params &p, const DevTables &t, bool fp64, long long pid_begin,
                     long long n, int num_sms, cudaStream_t stream);
+
+    // Batched solve: many instances in one queue (tables and outputs per instance).
+    cudaError_t run_batch(const std::vector<dsmc_params> &ps, const std::vector<DevTables> &ts,
+                          const std::vector<long long> &counts, int num_sms, cudaStream_t stream);
+
+    void set_shape(int blk, int per_sm, int k, int g) {
+        if (blk != block || per_sm != blocks_per_sm) nslots_want_changed_ = true;
+        block = blk;
+        blocks_per_sm = per_sm;
+        steps_per_launch = k;
+        launches_per_graph = g;
+    }
+    long long slot_count() const { return nslots_; }
+
+    // Launch shape (autotuned or set by the caller).
+    int block = 256;          // threads per block
+    int blocks_per_sm = 0;    // resident blocks per SM (0 = as many as fit)
+    int steps_per_launch = 2048;
+    int launches_per_graph = 8;
+    long long launches = 0;   // launches issued by the last run
+
+private:
+    cudaError_t ensure_slots(int num_sms);
+    cudaError_t upload_instances(const std::vector<dsmc_params> &ps,
+                                 const std::vector<DevTables> &ts,
+                                 const std::vector<long long> &counts,
+                                 const std::vector<long long> &pid_begins, cudaStream_t stream);
+    cudaError_t drain(long long total, cudaStream_t stream);
+    void free_all();
+
+    Slots slots_{};
+    void *slot_mem_ = nullptr;
+    long long nslots_ = 0;
+    FastInst *d_inst_ = nullptr;
+    int ninst_cap_ = 0;
+    int ninst_ = 0;
+    float *d_tab_ = nullptr;
+    size_t tab_cap_ = 0;
+    FastCounters *d_ctr_ = nullptr;
+    FastCounters *h_ctr_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+    cudaStream_t graph_stream_ = nullptr;
+    int graph_key_[4] = {0, 0, 0, 0};
+    bool nslots_want_changed_ = false;
 };
 
 }  // namespace dsmc

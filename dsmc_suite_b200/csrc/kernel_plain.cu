@@ -421,7 +421,46 @@ long long plain_blocks(long long n, int num_sms) {
     return blocks > cap ? cap : blocks;
 }
 
+// Fed-state push: integrate each (s, v) with the reference's Verlet variant for up to nsteps
+// steps, starting from oa = GM s / r^3 (ballistic.c:176-181), stopping at landing or escape.
+__global__ void push_fp64_kernel(const dsmc_params p, long long n, int nsteps, double *pos,
+                                 double *vel, int *status, int *taken) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    double v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+    const double h = p.dt_step;
+    double Ri = len3(s);
+    double oa[3];
+    for (int k = 0; k < 3; k++) oa[k] = p.GM * s[k] / (Ri * Ri * Ri);
+    int st = 0, k = 0;
+    for (; k < nsteps && st == 0; k++) {
+        const double R0 = len3(s);
+        const double g = p.GM / (R0 * R0 * R0);
+        const double h2 = h * h;
+        double ns[3];
+        for (int j = 0; j < 3; j++)
+            ns[j] = s[j] + v[j] * h - g * s[j] * (1.5 * h2) - oa[j] * (h2 / 6.0);
+        for (int j = 0; j < 3; j++) v[j] -= g * s[j] * h;
+        for (int j = 0; j < 3; j++) oa[j] = g * s[j];
+        s[0] = ns[0]; s[1] = ns[1]; s[2] = ns[2];
+        Ri = len3(s);
+        st = Ri <= p.Radii ? 1 : (Ri >= p.max_height ? 2 : 0);
+    }
+    for (int j = 0; j < 3; j++) { pos[3 * i + j] = s[j]; vel[3 * i + j] = v[j]; }
+    status[i] = st;
+    taken[i] = k;
+}
+
 }  // namespace
+
+cudaError_t launch_push_fp64(const dsmc_params &p, long long n, int nsteps, double *pos,
+                             double *vel, int *status, int *taken, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    push_fp64_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, stream>>>(p, n, nsteps, pos, vel,
+                                                                                status, taken);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_plain_fp64(const dsmc_params &p, const DevTables &t, long long pid_begin,
                               long long n, int num_sms, cudaStream_t stream) {

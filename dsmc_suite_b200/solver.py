@@ -137,6 +137,18 @@ class Context:
             N.ptr(box), N.ptr(total), N.ptr(valid, C.c_int32)), "fit hist")
         return coef, box, total, valid
 
+    def push(self, path: int, pos: np.ndarray, vel: np.ndarray, nsteps: int):
+        """Fed-state push of [n][3] positions/velocities (copies); returns (pos, vel, status,
+        steps_taken)."""
+        P = np.ascontiguousarray(pos, dtype=np.float64).copy()
+        V = np.ascontiguousarray(vel, dtype=np.float64).copy()
+        n = P.shape[0]
+        st = np.zeros(n, dtype=np.int32)
+        tk = np.zeros(n, dtype=np.int32)
+        self._check(self._lib.dsmc_push_host(self.h, path, n, nsteps, N.ptr(P), N.ptr(V),
+                                             N.ptr(st, C.c_int32), N.ptr(tk, C.c_int32)), "push")
+        return P, V, st, tk
+
     def velocity_record(self, n: int, per_bucket: int = 200, total_cap: int | None = None):
         p = self.params
         if total_cap is None:

@@ -122,6 +122,20 @@ int dsmc_zero(dsmc_ctx *ctx);
 int dsmc_run(dsmc_ctx *ctx, int path, int64_t pid_begin, int64_t n);
 int dsmc_sync(dsmc_ctx *ctx);
 
+/* Launch shape of the FAST paths: threads per block, resident blocks per SM (0 = as many as
+ * fit), Verlet steps per slot per launch, and launches per captured CUDA graph (1 = no graph).
+ * Results do not depend on the shape: every particle's trajectory is a function of its id and
+ * the deposits are integer sums. */
+int dsmc_set_launch_shape(dsmc_ctx *ctx, int block, int blocks_per_sm, int steps_per_launch,
+                          int launches_per_graph);
+/* Kernel launches issued by the last dsmc_run and the resident slot count of the FAST paths. */
+int dsmc_get_launch_info(dsmc_ctx *ctx, int64_t *launches, int64_t *nslots);
+
+/* Measured FMA throughput of this device [TFLOP/s] for FP32 (fp64 = 0) or FP64 (fp64 = 1):
+ * 8 independent FMA chains per thread over a few full waves, timed with CUDA events. The
+ * denominator of the push kernels' roofline fraction. */
+int dsmc_measure_fma_peak(dsmc_ctx *ctx, int fp64, double *tflops);
+
 /* Results (synchronous copies to host memory). */
 int dsmc_get_density(dsmc_ctx *ctx, uint64_t *density_fx);
 int dsmc_get_horizon(dsmc_ctx *ctx, uint64_t *horizon_fx);
@@ -132,6 +146,10 @@ int dsmc_get_speed_hist(dsmc_ctx *ctx, uint64_t *hist);
  * of the run that produced them. Any pointer may be NULL. */
 int dsmc_get_particle_outputs(dsmc_ctx *ctx, int64_t n, double *ttime, int32_t *fate,
                               int64_t *steps);
+/* Device-to-device copy of the fixed-point grids into caller buffers on the same device
+ * (asynchronous on the context stream), e.g. into communication buffers for a reduction across
+ * GPUs. Either destination may be NULL. */
+int dsmc_copy_grids_device(dsmc_ctx *ctx, uint64_t *density_dst, uint64_t *horizon_dst);
 /* Device address of the fixed-point density grid and its length in cells, for collectives. */
 int dsmc_density_device(dsmc_ctx *ctx, uint64_t **dev_ptr, int64_t *ncell);
 int dsmc_horizon_device(dsmc_ctx *ctx, uint64_t **dev_ptr, int64_t *ncell);
@@ -147,6 +165,16 @@ int dsmc_fit_cdf_samples_host(dsmc_ctx *ctx, int64_t ncell, int max_per_cell,
 int dsmc_fit_cdf_hist_host(dsmc_ctx *ctx, int64_t ncell, int nbins, double bin_width,
                            const uint64_t *hist, int degree, double *coef, double *box,
                            double *total, int32_t *valid);
+
+/* Fed-state push: integrate n particles from the given positions and velocities (host arrays
+ * [n][3], updated in place) with the reference's Verlet variant (verlet_step,
+ * src/common/integrator.c:4-55) and the context's GM, dt, Radii and max_height, for up to nsteps
+ * steps each, starting from oa = GM s / r^3 (src/dsmc/ballistic.c:176-181). A particle stops at
+ * landing (status 1) or escape (status 2); status 0 means it ran all nsteps. steps_taken may be
+ * NULL. PLAIN_FP64 (and FAST_FP64) use the FP64 arithmetic of the plain kernel; FAST_FP32 uses
+ * the compensated FP32 push of the fast path. */
+int dsmc_push_host(dsmc_ctx *ctx, int path, int64_t n, int nsteps, double *pos, double *vel,
+                   int32_t *status, int32_t *steps_taken);
 
 /* Velocity record of the ballistic runner (src/dsmc/ballistic.c:216-232): for each
  * (latitude row, shell) bucket, the first per_bucket visits in (particle id, step) order, i.e.

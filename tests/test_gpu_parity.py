@@ -1,0 +1,284 @@
+"""Parity of the CUDA paths with the oracle, through the C ABI (needs a B200).
+
+Bars:
+  * plain FP64 path vs oracle on identical Philox streams: bit-identical fixed-point grids and
+    per-particle fates and step counts; the only allowed differences come from CUDA's and
+    glibc's transcendentals (asin, atan2, sin, cos, log, exp) rounding differently in the last
+    place, so a small fraction of particles may take a different branch (<= 0.5%), and the
+    per-particle float rows agree to 1e-9 relative;
+  * fed-state FP64 push: bit-identical to the reference's verlet_step;
+  * FP32 compensated push: end-point position error <= 1 m after 2000 steps (<= 1e-6 relative
+    to the ~1e6 m path);
+  * fits on the device: bit-identical to the oracle's FP64 fits;
+  * FAST_FP32 vs plain FP64: deterministic (bit-identical across runs and launch shapes) and
+    within the density relative-L2 stated at each test."""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, cold_T
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel_l1(a, b):
+    a = a.astype(np.float64)
+    b = b.astype(np.float64)
+    return np.abs(a - b).sum() / max(np.abs(b).sum(), 1.0)
+
+
+def _compare_plain_vs_oracle(g, o, n):
+    differing = np.count_nonzero((g["fate"] != o["fate"]) | (g["steps"] != o["steps"]))
+    assert differing <= max(1, 0.005 * n), differing
+    assert _rel_l1(g["density"], o["density"]) <= 1e-3
+    assert _rel_l1(g["horizon"], o["horizon"]) <= 1e-2
+    same = (g["fate"] == o["fate"]) & (g["steps"] == o["steps"])
+    np.testing.assert_allclose(g["ttime"][:, same], o["ttime"][:, same], rtol=1e-9, atol=1e-6)
+    if differing == 0:
+        np.testing.assert_array_equal(g["density"], o["density"])
+        np.testing.assert_array_equal(g["horizon"], o["horizon"])
+
+
+def test_plain_reference_ballistic_vs_oracle(ctx, N, O):
+    p = N.params_reference(N.RUNNER_BALLISTIC, 36, 72)
+    S = N.SurfaceInputs(T_map=cold_T(N))
+    n = 3000
+    g = ctx.solve(N.PATH_PLAIN_FP64, p, S, n, outputs=True)
+    o = O.run(p, S, n, nthreads=4)
+    _compare_plain_vs_oracle(g, o, n)
+    assert g["stats"]["total_steps"] == o["total_steps"] or \
+        abs(g["stats"]["total_steps"] - o["total_steps"]) < 1e-3 * o["total_steps"]
+    assert (o["fate"] == N.FATE_FROZEN).sum() > 0      # the freeze paths were exercised
+
+
+def test_plain_reference_advanced_vs_oracle(ctx, N, O, golden):
+    from test_oracle_golden import _reference_advanced_inputs
+    p, col, _ = _reference_advanced_inputs(N, O, golden)
+    S = N.SurfaceInputs(T_map=golden["runs"]["T"])
+    n = 1500
+    g = ctx.solve(N.PATH_PLAIN_FP64, p, S, n, collision=col, outputs=True)
+    o = O.run(p, S, n, collision=col, nthreads=4)
+    assert o["n_collisions"] > 1000
+    assert abs(g["stats"]["n_collisions"] - o["n_collisions"]) <= 0.01 * o["n_collisions"]
+    _compare_plain_vs_oracle(g, o, n)
+
+
+@pytest.fixture(scope="module")
+def config_surface(N):
+    ico = N.Icosphere(3)
+    return N.SurfaceInputs(ico=ico, face_T=ico.face_temperature())
+
+
+def test_plain_config_ballistic_vs_oracle(ctx, N, O, config_surface):
+    p = N.params_config(N.RUNNER_BALLISTIC)
+    n = 3000
+    g = ctx.solve(N.PATH_PLAIN_FP64, p, config_surface, n, outputs=True)
+    o = O.run(p, config_surface, n, nthreads=4)
+    _compare_plain_vs_oracle(g, o, n)
+    fates = np.bincount(o["fate"], minlength=5)
+    assert fates[N.FATE_ESCAPED] > 0 and fates[N.FATE_FROZEN] > 0 and fates[N.FATE_STEP_CAP] > 0
+
+
+def _config_collision_inputs(ctx, N, O, surface, n_phase1=20000, scale=1e10):
+    """Phase 1 on the GPU with speed histograms, FP64 fits on the device, background scaled so
+    collisions fire. Returns (params_phase2, CollisionInputs, fits)."""
+    p1 = N.params_config(N.RUNNER_BALLISTIC)
+    p1.n_speed_bins = 64
+    ctx.setup(p1, surface)
+    ctx.zero()
+    ctx.run(N.PATH_PLAIN_FP64, 0, n_phase1)
+    ctx.sync()
+    hist = ctx.speed_hist()
+    den = ctx.density().astype(np.float64) / N.FIXED_SCALE
+    coef, box, total, valid = ctx.fit_hist(hist, p1.speed_bin_width, 6)
+    # the fits are laid out [td][fd][ht] like the reference's poly_mat
+    hd, ftd, ffd = p1.hd, p1.ftd, p1.ffd
+    reord = lambda a: a.reshape(hd, ftd, ffd, -1).transpose(1, 2, 0, 3).reshape(hd * ftd * ffd, -1)
+    col = N.CollisionInputs(den.ravel() * scale, reord(coef), reord(box), reord(total[:, None]).ravel(),
+                            reord(valid[:, None]).ravel(), 6)
+    p2 = N.params_config(N.RUNNER_ADVANCED)
+    return p2, col, (hist, coef, box, total, valid)
+
+
+def test_plain_config_advanced_vs_oracle(ctx, N, O, config_surface):
+    p2, col, _ = _config_collision_inputs(ctx, N, O, config_surface)
+    n = 1500
+    g = ctx.solve(N.PATH_PLAIN_FP64, p2, config_surface, n, collision=col, outputs=True)
+    o = O.run(p2, config_surface, n, collision=col, nthreads=4)
+    assert o["n_collisions"] > 100
+    _compare_plain_vs_oracle(g, o, n)
+
+
+def test_speed_hist_and_fits_vs_oracle(ctx, N, O, config_surface):
+    p1 = N.params_config(N.RUNNER_BALLISTIC)
+    p1.n_speed_bins = 64
+    n = 2000
+    ctx.setup(p1, config_surface)
+    ctx.zero()
+    ctx.run(N.PATH_PLAIN_FP64, 0, n)
+    ctx.sync()
+    hist = ctx.speed_hist()
+    o = O.run(p1, config_surface, n, nthreads=4, speed_hist=True)
+    assert _rel_l1(hist, o["speed_hist"]) <= 1e-3
+    coef, box, total, valid = ctx.fit_hist(o["speed_hist"], p1.speed_bin_width, 6)
+    L = O.lib()
+    checked = 0
+    for k in np.nonzero(o["speed_hist"].sum(axis=1) > 8)[0][:3000]:
+        c8, b4, t1 = np.zeros(8), np.zeros(4), np.zeros(1)
+        h = np.ascontiguousarray(o["speed_hist"][k])
+        ok = L.or_fit_cell_from_hist(h.ctypes.data_as(C.POINTER(C.c_uint64)), 64,
+                                     p1.speed_bin_width, 6, O._p(c8), O._p(b4), O._p(t1))
+        assert ok == valid[k]
+        if ok:
+            np.testing.assert_array_equal(coef[k], c8)
+            np.testing.assert_array_equal(box[k], b4)
+            checked += 1
+    assert checked > 100
+
+
+def test_fit_samples_vs_oracle(ctx, N, O, golden):
+    from test_oracle_golden import _reference_advanced_inputs
+    p, col, (sp, cnt) = _reference_advanced_inputs(N, O, golden)
+    coef, box, total, valid = ctx.fit_samples(sp, cnt, 3)
+    np.testing.assert_array_equal(valid, col.valid)
+    np.testing.assert_array_equal(coef[valid == 1], col.coef[valid == 1])
+    np.testing.assert_array_equal(box[valid == 1], col.box[valid == 1])
+    np.testing.assert_array_equal(total, col.total)
+
+
+def test_fed_state_push_fp64_matches_reference(ctx, N, golden):
+    g = golden["scalars"]
+    p = N.params_reference(N.RUNNER_BALLISTIC, 36, 72)
+    p.GM = float(g["verlet_GM"])
+    p.dt_step = float(g["verlet_h"])
+    p.max_height = float(g["verlet_max_height"])
+    ctx.setup(p, N.SurfaceInputs(T_map=cold_T(N)))
+    P, V, st, tk = ctx.push(N.PATH_PLAIN_FP64, g["verlet_s0"], g["verlet_v0"], int(g["verlet_steps"]))
+    np.testing.assert_array_equal(st, g["verlet_status"])
+    np.testing.assert_array_equal(tk, g["verlet_taken"])
+    np.testing.assert_array_equal(P, g["verlet_s"])
+    np.testing.assert_array_equal(V, g["verlet_v"])
+
+
+def _seeded_states(p, m=10000, seed=1):
+    rng = np.random.default_rng(seed)
+    th = np.arcsin(rng.uniform(-1, 1, m))
+    ph = rng.uniform(0, 2 * np.pi, m)
+    r = p.Radii * rng.uniform(1.001, 1.5, m)
+    pos = np.stack([r * np.cos(th) * np.sin(ph), r * np.cos(th) * np.cos(ph), r * np.sin(th)], 1)
+    vel = rng.normal(0, 120, (m, 3)) + pos / np.linalg.norm(pos, axis=1)[:, None] * 250
+    return pos, vel
+
+
+def test_fed_state_push_fp32_endpoint_error(ctx, N, config_surface):
+    p = N.params_config(N.RUNNER_BALLISTIC)
+    ctx.setup(p, config_surface)
+    pos, vel = _seeded_states(p)
+    P64, V64, s64, t64 = ctx.push(N.PATH_PLAIN_FP64, pos, vel, 2000)
+    P32, V32, s32, t32 = ctx.push(N.PATH_FAST_FP32, pos, vel, 2000)
+    same = (s64 == s32) & (t64 == t32)
+    assert same.mean() > 0.999
+    err = np.linalg.norm(P32 - P64, axis=1)[same]
+    assert err.max() <= 1.0, err.max()          # metres, after up to 2000 steps of 2 s
+    assert np.median(err) <= 0.1
+
+
+def test_velocity_record_vs_oracle(ctx, N, O):
+    p = N.params_reference(N.RUNNER_BALLISTIC, 36, 72)
+    S = N.SurfaceInputs(T_map=cold_T(N))
+    n = 400
+    ctx.setup(p, S)
+    v, td, fd, ht = ctx.velocity_record(n)
+    o = O.run(p, S, n, nthreads=1, v_record=True, particles=False)
+    k = min(len(v), o["n_records"])
+    assert abs(len(v) - o["n_records"]) <= 0.005 * o["n_records"] + 1
+    assert len(v) > 1000
+    agree = (td[:k] == o["v_td"][:k]) & (fd[:k] == o["v_fd"][:k]) & (ht[:k] == o["v_ht"][:k])
+    assert agree.mean() > 0.99
+    np.testing.assert_allclose(v[:k][agree], o["v_record"][:k][agree], rtol=1e-9)
+
+
+def test_fast_path_is_deterministic_across_launch_shapes(ctx, N, config_surface):
+    p = N.params_config(N.RUNNER_BALLISTIC)
+    n = 50000
+    outs = []
+    for shape in ((256, 0, 2048, 8), (128, 2, 300, 1), (256, 1, 7000, 3)):
+        N.check(N.lib().dsmc_set_launch_shape(ctx.h, *shape), "shape", ctx.h)
+        r = ctx.solve(N.PATH_FAST_FP32, p, config_surface, n, outputs=True)
+        outs.append(r)
+    N.check(N.lib().dsmc_set_launch_shape(ctx.h, 256, 0, 2048, 8), "shape", ctx.h)
+    for r in outs[1:]:
+        np.testing.assert_array_equal(r["density"], outs[0]["density"])
+        np.testing.assert_array_equal(r["horizon"], outs[0]["horizon"])
+        np.testing.assert_array_equal(r["steps"], outs[0]["steps"])
+        assert r["stats"] == outs[0]["stats"]
+
+
+@pytest.mark.parametrize("model", ["config", "reference"])
+def test_fast_fp32_vs_plain_fp64(ctx, N, config_surface, model):
+    """Same Philox streams, FP32 compensated vs FP64: trajectories stay correlated, so the
+    density difference is far below the Monte Carlo noise of an independent run."""
+    if model == "config":
+        p, S = N.params_config(N.RUNNER_BALLISTIC), config_surface
+    else:
+        p, S = N.params_reference(N.RUNNER_BALLISTIC, 36, 72), N.SurfaceInputs(T_map=cold_T(N))
+    n = 100000
+    a = ctx.solve(N.PATH_PLAIN_FP64, p, S, n, outputs=True)
+    b = ctx.solve(N.PATH_FAST_FP32, p, S, n, outputs=True)
+    q = p.copy()
+    q.seed = p.seed + 1
+    c = ctx.solve(N.PATH_PLAIN_FP64, q, S, n)
+    da, db, dc = (x["density"].astype(np.float64) for x in (a, b, c))
+    rel = np.linalg.norm(db - da) / np.linalg.norm(da)
+    noise = np.linalg.norm(dc - da) / np.linalg.norm(da)
+    assert rel < 0.25 * noise, (rel, noise)
+    assert abs(b["stats"]["total_steps"] / a["stats"]["total_steps"] - 1) < 1e-3
+    assert np.mean(a["fate"] == b["fate"]) > 0.99
+
+
+def test_runner_files_match_oracle(N, O, tmp_path, built):
+    """The drop-in CLI (`dsmc_suite dsmc`) writes the reference's files; its density equals the
+    oracle's fixed-point grid to the printed precision and its velocity record to %f."""
+    T = cold_T(N)
+    (tmp_path / "T.dat").write_text("36\n72\n" + "".join(f"{x:.17g}\n" for x in T.ravel()))
+    cli = ROOT / "dsmc_suite_b200" / "bin" / "dsmc_suite"
+    n = 300
+    r = subprocess.run([str(cli), "dsmc", "-n", str(n), "-T", str(tmp_path / "T.dat"), "-o",
+                        str(tmp_path / "g")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "Simulation complete" in r.stdout
+    p = N.params_reference(N.RUNNER_BALLISTIC, 36, 72)
+    o = O.run(p, N.SurfaceInputs(T_map=T), n, nthreads=1, v_record=True)
+    den = np.array((tmp_path / "g_den.dat").read_text().split()[3:], dtype=np.float64)
+    np.testing.assert_allclose(den, o["density"].ravel() / N.FIXED_SCALE, atol=1.5e-6)
+    vr = (tmp_path / "g_v_record.dat").read_text().split()
+    assert abs(int(vr[0]) - o["n_records"]) <= 0.01 * o["n_records"] + 1
+    tt = np.array((tmp_path / "g_ttime.dat").read_text().split(), dtype=np.float64).reshape(5, n)
+    np.testing.assert_allclose(tt, o["ttime"][:5], atol=2e-5)
+    # phase 2 consumes the phase-1 files
+    r = subprocess.run([str(cli), "dsmc-adv", "-n", "200", "-T", str(tmp_path / "T.dat"), "-d",
+                        str(tmp_path / "g_den.dat"), "-v", str(tmp_path / "g_v_record.dat"), "-o",
+                        str(tmp_path / "h")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "Valid polynomial fits" in r.stdout and (tmp_path / "h_ttime.dat").exists()
+
+
+def test_abi_error_paths(N, built):
+    from dsmc_suite_b200 import Context, DsmcError
+    with Context(0) as c:
+        with pytest.raises(DsmcError) as e:
+            c.run(N.PATH_PLAIN_FP64, 0, 10)
+        assert e.value.status == -5              # run before setup
+        p = N.params_config(N.RUNNER_BALLISTIC)
+        with pytest.raises(DsmcError):
+            c.setup(p, N.SurfaceInputs(T_map=np.zeros((36, 72))))   # config model, no icosphere
+        bad = N.params_reference(N.RUNNER_BALLISTIC, 36, 72)
+        bad.dt_step = -1.0
+        with pytest.raises(DsmcError):
+            c.setup(bad, N.SurfaceInputs(T_map=np.zeros((36, 72))))
+        with pytest.raises(DsmcError):
+            N.check(N.lib().dsmc_set_launch_shape(c.h, 100, 0, 10, 1), "shape", c.h)
