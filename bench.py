@@ -215,7 +215,10 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=900),
                                 device_id=torch.device("cuda", local))
-    stream = torch.cuda.current_stream()
+    # One dedicated stream for the library's kernels, the L2 flush and the timing events (the
+    # legacy default stream has handle 0, which the C ABI reads as "the context's own stream").
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = Context(local)
     ctx.set_stream(stream.cuda_stream)
     p, S = config_problem(N)
