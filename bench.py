@@ -47,6 +47,8 @@ def args_parse():
     ap.add_argument("--plain-particles", type=float, default=1e7,
                     help="particles of the plain FP64 comparison solve (rank 0, N=1)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--shape", type=str, default=None,
+                    help="launch shape block,blocks_per_sm,steps_per_launch,launches_per_graph")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -225,6 +227,10 @@ def main():
     n = int(a.particles)
     pid0 = rank * n
     ctx.setup(p, S)
+    if a.shape:
+        shape = [int(v) for v in a.shape.split(",")]
+        N.check(N.lib().dsmc_set_launch_shape(ctx.h, *shape), "launch shape", ctx.h)
+        CONFIG["launch_shape"] = shape
     ncell, nh = p.ncell, p.ftd * p.ffd
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     red = torch.zeros(ncell + nh, dtype=torch.int64, device="cuda") if world > 1 else None

@@ -1,13 +1,14 @@
 // fast_engine.cu - the FAST_FP32 path: resident particle slots, a device work queue, an FP32
-// push with two-sum compensated position and velocity, cell tracking by comparisons, and
-// register run-length deposits flushed as 64-bit fixed-point atomics.
+// push with two-sum compensated position and velocity, cell tracking by comparisons against
+// register-cached cell bounds, and per-cell register accumulation of the fixed-point deposits.
 //
 // Per step the hot loop does one gravity evaluation (one rsqrt), the reference's Verlet variant
 // (src/common/integrator.c:21-44) with the position and velocity sums kept as (hi, lo) float
-// pairs, shell/latitude/longitude tracking against precomputed boundary tables (no asin, atan2
-// or log), photolysis as W0 * 2^(-c * n_day) (one ex2), and a deposit into the register run.
-// Rare events (launch, landing, collision, end of life) leave the loop for code that works in
-// FP32 with FP64 where the reference's classification needs it (launch energy).
+// pairs, an in-cell test against the eight bounds of the current cell held in registers (no
+// asin, atan2, log or table load), photolysis as W0 * 2^(-c * n_day) (one ex2), and the deposit
+// into the register accumulator of the current cell, flushed with one 64-bit atomic when the
+// particle leaves the cell. Rare events (cell change, launch, landing, collision, end of life)
+// leave the loop for code that reads the boundary tables and the cold per-particle fields.
 #include "fast_engine.h"
 #include "dsmc_kernels.h"
 
@@ -41,100 +42,96 @@ struct FastArgs {
     int K;
 };
 
-// Per-thread working copy of one slot.
-struct Reg {
-    int inst;
-    unsigned pid, evt;
+// Register-resident state of the particle a thread pushes. The cold fields (particle id, Philox
+// event counter, collision count, freeze waiting time) stay in the slot arrays.
+struct Hot {
     float sh[3], sl[3], vh[3], vl[3], oa[3];
-    float w0;
-    int nday, steps, hop, cell, run_cell;
-    unsigned long long run_acc;
+    float w0, pcol, pthr, nsig;
+    int nday, steps, hop;
+    int cell;                  // packed (ht << 16) | (td << 8) | fd
+    int ci;                    // (ht * ftd + td) * ffd + fd, -1 = none
+    unsigned long long acc;    // fixed-point deposits of cell ci not yet flushed
     int hist_key, hist_cnt;
-    float pcol, pthr;
-    int ncol;
-    float rest, thi0;
+    int inst;                  // -1 = empty slot
 };
 
-__device__ __forceinline__ void load_slot(const Slots &s, long long i, long long S, Reg &r) {
-    r.inst = s.inst[i];
-    r.pid = s.pid[i];
-    r.evt = s.evt[i];
+// Bounds of the current cell: r^2 in (r2lo, r2hi], z|z| in (r^2 zlo, r^2 zhi], longitude between
+// the directions (s0, c0) and (s1, c1).
+struct Bounds {
+    float r2lo, r2hi, zlo, zhi, s0, c0, s1, c1;
+};
+
+__device__ __forceinline__ void load_hot(const Slots &s, long long i, long long S, Hot &h) {
+    h.inst = s.inst[i];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        r.sh[k] = s.sh[k * S + i];
-        r.sl[k] = s.sl[k * S + i];
-        r.vh[k] = s.vh[k * S + i];
-        r.vl[k] = s.vl[k * S + i];
-        r.oa[k] = s.oa[k * S + i];
+        h.sh[k] = s.sh[k * S + i];
+        h.sl[k] = s.sl[k * S + i];
+        h.vh[k] = s.vh[k * S + i];
+        h.vl[k] = s.vl[k * S + i];
+        h.oa[k] = s.oa[k * S + i];
     }
-    r.w0 = s.w0[i];
-    r.nday = s.nday[i];
-    r.steps = s.steps[i];
-    r.hop = s.hop[i];
-    r.cell = s.cell[i];
-    r.run_cell = s.run_cell[i];
-    r.run_acc = s.run_acc[i];
-    r.hist_key = s.hist_key[i];
-    r.hist_cnt = s.hist_cnt[i];
-    r.pcol = s.pcol[i];
-    r.pthr = s.pthr[i];
-    r.ncol = s.ncol[i];
-    r.rest = s.rest[i];
-    r.thi0 = s.thi0[i];
+    h.w0 = s.w0[i];
+    h.nday = s.nday[i];
+    h.steps = s.steps[i];
+    h.hop = s.hop[i];
+    h.cell = s.cell[i];
+    h.ci = s.run_cell[i];
+    h.acc = s.run_acc[i];
+    h.hist_key = s.hist_key[i];
+    h.hist_cnt = s.hist_cnt[i];
+    h.pcol = s.pcol[i];
+    h.pthr = s.pthr[i];
+    h.nsig = 0.0f;
 }
 
-__device__ __forceinline__ void store_slot(const Slots &s, long long i, long long S, const Reg &r) {
-    s.inst[i] = r.inst;
-    s.pid[i] = r.pid;
-    s.evt[i] = r.evt;
+__device__ __forceinline__ void store_hot(const Slots &s, long long i, long long S, const Hot &h) {
+    s.inst[i] = h.inst;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        s.sh[k * S + i] = r.sh[k];
-        s.sl[k * S + i] = r.sl[k];
-        s.vh[k * S + i] = r.vh[k];
-        s.vl[k * S + i] = r.vl[k];
-        s.oa[k * S + i] = r.oa[k];
+        s.sh[k * S + i] = h.sh[k];
+        s.sl[k * S + i] = h.sl[k];
+        s.vh[k * S + i] = h.vh[k];
+        s.vl[k * S + i] = h.vl[k];
+        s.oa[k * S + i] = h.oa[k];
     }
-    s.w0[i] = r.w0;
-    s.nday[i] = r.nday;
-    s.steps[i] = r.steps;
-    s.hop[i] = r.hop;
-    s.cell[i] = r.cell;
-    s.run_cell[i] = r.run_cell;
-    s.run_acc[i] = r.run_acc;
-    s.hist_key[i] = r.hist_key;
-    s.hist_cnt[i] = r.hist_cnt;
-    s.pcol[i] = r.pcol;
-    s.pthr[i] = r.pthr;
-    s.ncol[i] = r.ncol;
-    s.rest[i] = r.rest;
-    s.thi0[i] = r.thi0;
+    s.w0[i] = h.w0;
+    s.nday[i] = h.nday;
+    s.steps[i] = h.steps;
+    s.hop[i] = h.hop;
+    s.cell[i] = h.cell;
+    s.run_cell[i] = h.ci;
+    s.run_acc[i] = h.acc;
+    s.hist_key[i] = h.hist_key;
+    s.hist_cnt[i] = h.hist_cnt;
+    s.pcol[i] = h.pcol;
+    s.pthr[i] = h.pthr;
 }
 
-__device__ __forceinline__ void set_pos(Reg &r, const double s[3]) {
+__device__ __forceinline__ void set_pos(Hot &h, const double s[3]) {
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        r.sh[k] = static_cast<float>(s[k]);
-        r.sl[k] = static_cast<float>(s[k] - static_cast<double>(r.sh[k]));
+        h.sh[k] = static_cast<float>(s[k]);
+        h.sl[k] = static_cast<float>(s[k] - static_cast<double>(h.sh[k]));
     }
 }
 
-__device__ __forceinline__ void set_vel(Reg &r, const double v[3]) {
+__device__ __forceinline__ void set_vel(Hot &h, const double v[3]) {
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        r.vh[k] = static_cast<float>(v[k]);
-        r.vl[k] = static_cast<float>(v[k] - static_cast<double>(r.vh[k]));
+        h.vh[k] = static_cast<float>(v[k]);
+        h.vl[k] = static_cast<float>(v[k] - static_cast<double>(h.vh[k]));
     }
 }
 
-__device__ __forceinline__ void get_pos(const Reg &r, double s[3]) {
+__device__ __forceinline__ void get_pos(const Hot &h, double s[3]) {
 #pragma unroll
-    for (int k = 0; k < 3; k++) s[k] = static_cast<double>(r.sh[k]) + static_cast<double>(r.sl[k]);
+    for (int k = 0; k < 3; k++) s[k] = static_cast<double>(h.sh[k]) + static_cast<double>(h.sl[k]);
 }
 
-__device__ __forceinline__ void get_vel(const Reg &r, double v[3]) {
+__device__ __forceinline__ void get_vel(const Hot &h, double v[3]) {
 #pragma unroll
-    for (int k = 0; k < 3; k++) v[k] = static_cast<double>(r.vh[k]) + static_cast<double>(r.vl[k]);
+    for (int k = 0; k < 3; k++) v[k] = static_cast<double>(h.vh[k]) + static_cast<double>(h.vl[k]);
 }
 
 __device__ __forceinline__ int pack_cell(int ht, int td, int fd) { return (ht << 16) | (td << 8) | fd; }
@@ -143,8 +140,8 @@ __device__ __forceinline__ int pack_cell(int ht, int td, int fd) { return (ht <<
 // current (td, fd) by boundary comparisons. Row td covers latitudes (b_td, b_td+1] and column fd
 // longitudes (phi_fd, phi_fd+1], the upper-inclusive cells of grid_spherical_to_index
 // (src/common/grid.c:28-39).
-__device__ __forceinline__ void track_angles(const FastInst &I, float x, float y, float z, float r2,
-                                             int &td, int &fd) {
+__device__ void track_angles(const FastInst &I, float x, float y, float z, float r2, int &td,
+                             int &fd) {
     const int ftd = I.p.ftd, ffd = I.p.ffd;
     const float zz = z * fabsf(z);
     for (int it = 0; it < 64 && td + 1 < ftd && zz > r2 * __ldg(I.sbs + td + 1); it++) td++;
@@ -161,26 +158,25 @@ __device__ __forceinline__ void track_angles(const FastInst &I, float x, float y
     }
 }
 
-__device__ __forceinline__ void track_shell(const FastInst &I, float r2, int &ht) {
+__device__ void track_shell(const FastInst &I, float r2, int &ht) {
     const int hd = I.p.hd;
     for (int it = 0; it < 64 && ht + 1 < hd && r2 > __ldg(I.rb2 + ht + 1); it++) ht++;
     for (int it = 0; it < 64 && ht > 0 && r2 <= __ldg(I.rb2 + ht); it++) ht--;
 }
 
 // Cell of a position from scratch: an estimate from the angles, then the comparison fix-up.
-__device__ void cell_from_scratch(const FastInst &I, const float x, const float y, const float z,
-                                  int &ht, int &td, int &fd) {
+__device__ int cell_from_scratch(const FastInst &I, const float x, const float y, const float z) {
     const float r2 = x * x + y * y + z * z;
     const float r = sqrtf(r2);
-    float th = asinf(fminf(1.0f, fmaxf(-1.0f, z / r)));
+    const float th = asinf(fminf(1.0f, fmaxf(-1.0f, z / r)));
     float ph = atan2f(x, y);
     if (ph < 0.0f) ph += 2.0f * kPiF;
-    td = static_cast<int>((th + 0.5f * kPiF) / kPiF * I.p.ftd);
-    fd = static_cast<int>(ph / (2.0f * kPiF) * I.p.ffd);
+    int td = static_cast<int>((th + 0.5f * kPiF) / kPiF * I.p.ftd);
+    int fd = static_cast<int>(ph / (2.0f * kPiF) * I.p.ffd);
     td = min(max(td, 0), I.p.ftd - 1);
     fd = min(max(fd, 0), I.p.ffd - 1);
     track_angles(I, x, y, z, r2, td, fd);
-    ht = 0;
+    int ht;
     if (I.p.use_exp_grid) {
         const double arg = I.p.alpha2 * (static_cast<double>(r) - I.p.Radii) / I.p.unih + 1.0;
         ht = arg <= 1.0 ? 0 : static_cast<int>(log(arg) / I.p.log1p_alpha2);
@@ -189,6 +185,41 @@ __device__ void cell_from_scratch(const FastInst &I, const float x, const float 
     }
     ht = min(max(ht, 0), I.p.hd - 1);
     track_shell(I, r2, ht);
+    return pack_cell(ht, td, fd);
+}
+
+__device__ __forceinline__ void flush_cell(const FastInst &I, Hot &h) {
+    if (h.ci >= 0 && h.acc) atomicAdd(&I.t.density[h.ci], h.acc);
+    h.acc = 0;
+}
+
+__device__ __forceinline__ void flush_hist(const FastInst &I, Hot &h) {
+    if (h.hist_key >= 0 && h.hist_cnt)
+        atomicAdd(&I.t.speed_hist[h.hist_key], static_cast<unsigned long long>(h.hist_cnt));
+    h.hist_key = -1;
+    h.hist_cnt = 0;
+}
+
+// Makes `cell` the current cell: flushes the previous cell's deposits, loads the eight bounds
+// and the collision rate n * sigma of the new cell.
+__device__ void enter_cell(const FastInst &I, Hot &h, Bounds &b, int cell) {
+    flush_cell(I, h);
+    const int ht = cell >> 16, td = (cell >> 8) & 0xff, fd = cell & 0xff;
+    h.cell = cell;
+    h.ci = (ht * I.p.ftd + td) * I.p.ffd + fd;
+    b.r2lo = __ldg(I.rb2 + ht);
+    b.r2hi = __ldg(I.rb2 + ht + 1);
+    b.zlo = __ldg(I.sbs + td);
+    b.zhi = __ldg(I.sbs + td + 1);
+    const float2 lo = __ldg(I.lonb + fd), hi = __ldg(I.lonb + fd + 1);
+    b.s0 = lo.x;
+    b.c0 = lo.y;
+    b.s1 = hi.x;
+    b.c1 = hi.y;
+    h.nsig = 0.0f;
+    if (I.t.n_bg && I.p.runner == DSMC_RUNNER_ADVANCED && ht < I.p.collide_ht_max &&
+        h.ci < I.t.n_bg_len)
+        h.nsig = static_cast<float>(__ldg(I.t.n_bg + h.ci) * I.p.cross_section);
 }
 
 __device__ __forceinline__ double cdf_eval(const double *coef, const double *box, int degree,
@@ -243,45 +274,75 @@ __device__ void flush_stats(const FastArgs &a, StatAcc &st) {
 #pragma unroll
     for (int k = 0; k < 5; k++) {
         const unsigned sum = __reduce_add_sync(group, v[k]);
-        if (leader && key >= 0 && sum) atomicAdd(&a.inst[key].t.stats[slot_of[k]], static_cast<unsigned long long>(sum));
+        if (leader && key >= 0 && sum)
+            atomicAdd(&a.inst[key].t.stats[slot_of[k]], static_cast<unsigned long long>(sum));
     }
     st = StatAcc{};
 }
 
-__device__ __forceinline__ void flush_run(const FastInst &I, Reg &r) {
-    if (r.run_cell >= 0 && r.run_acc) atomicAdd(&I.t.density[r.run_cell], r.run_acc);
-    r.run_cell = -1;
-    r.run_acc = 0;
-    if (r.hist_key >= 0 && r.hist_cnt) atomicAdd(&I.t.speed_hist[r.hist_key], static_cast<unsigned long long>(r.hist_cnt));
-    r.hist_key = -1;
-    r.hist_cnt = 0;
+// The previous instance's share of the counters, lane by lane (an instance switch inside a
+// launch happens at most once per particle and is rare).
+__device__ void flush_stats_lane(const FastArgs &a, StatAcc &st) {
+    if (st.inst >= 0) {
+        unsigned long long *dst = a.inst[st.inst].t.stats;
+        if (st.steps) atomicAdd(dst + kStatSteps, static_cast<unsigned long long>(st.steps));
+        if (st.escaped) atomicAdd(dst + kStatEscaped, static_cast<unsigned long long>(st.escaped));
+        if (st.collisions) atomicAdd(dst + kStatCollisions, static_cast<unsigned long long>(st.collisions));
+        if (st.bound) atomicAdd(dst + kStatBound, static_cast<unsigned long long>(st.bound));
+        if (st.finished) {
+            atomicAdd(dst + kStatFinished, static_cast<unsigned long long>(st.finished));
+            atomicAdd(&a.ctr->finished, static_cast<unsigned long long>(st.finished));
+        }
+    }
+    st = StatAcc{};
 }
 
-__device__ __forceinline__ float weight(const FastInst &I, const Reg &r) {
-    return r.w0 * exp2f(-I.c_day * static_cast<float>(r.nday));
+__device__ __forceinline__ float weight(const FastInst &I, const Hot &h) {
+    return h.w0 * exp2f(-I.c_day * static_cast<float>(h.nday));
 }
 
-// Launch from the current surface position. Returns false when the reference's launch-speed
-// escape test fires (the particle ends as escaped).
-__device__ bool launch(const FastInst &I, Reg &r, StatAcc &st, float local_T, float thi, float fi) {
+__device__ __forceinline__ void ref_index(float thi, float fi, int ftd, int ffd, int &td, int &fd) {
+    td = static_cast<int>(ceilf((thi + 0.5f * kPiF) / kPiF * ftd)) - 1;
+    fd = static_cast<int>(ceilf(fi / (2.0f * kPiF) * ffd)) - 1;
+    td = min(max(td, 0), ftd - 1);
+    fd = min(max(fd, 0), ffd - 1);
+}
+
+__device__ __forceinline__ void angles_of(const Hot &h, float &thi, float &fi) {
+    double s[3];
+    get_pos(h, s);
+    const double R = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    thi = static_cast<float>(asin(s[2] / R));
+    double f = atan2(s[0], s[1]);
+    if (f < 0) f += 2.0 * kPi;
+    fi = static_cast<float>(f);
+}
+
+__device__ __forceinline__ void horizon_add(const FastInst &I, int td, int fd, float W) {
+    atomicAdd(&I.t.horizon[td * I.p.ffd + fd], __float2ull_rn(W * 16777216.0f));
+}
+
+// Launch from the current surface position (ballistic.c:156-181; config: flux-weighted
+// Maxwell-Boltzmann). Returns false when the reference's launch-speed escape test fires.
+__device__ bool launch(const FastArgs &a, long long i, const FastInst &I, Hot &h, StatAcc &st,
+                       float local_T, float thi, float fi) {
     const dsmc_params &p = I.p;
     Philox rng;
-    rng.init(p.seed, p.instance, r.pid);
-    rng.event = r.evt;
+    rng.init(p.seed, p.instance, a.s.pid[i]);
+    rng.event = a.s.evt[i];
     rng.next();
-    r.evt = rng.event;
+    a.s.evt[i] = rng.event;
     double s[3];
-    get_pos(r, s);
+    get_pos(h, s);
     float v[3];
     if (p.model == DSMC_MODEL_REFERENCE) {
-        // ballistic.c:125,156-173 in FP32
         const float KF = 2.0f * kPiF * static_cast<float>(p.Radii) * fabsf(cosf(thi)) / static_cast<float>(p.P);
         int idx = local_T >= 220.0f ? 20 : static_cast<int>(ceilf(local_T / 10.0f)) - 2;
         idx = idx < 0 ? 0 : (idx >= 23 ? 22 : idx);
         const float vr = static_cast<float>(I.t.vt_speeds[idx * 1000 + rng.w[0] % static_cast<uint32_t>(I.t.vt_count[idx])]);
         float vold2 = 0.0f;
 #pragma unroll
-        for (int k = 0; k < 3; k++) vold2 += r.vh[k] * r.vh[k];
+        for (int k = 0; k < 3; k++) vold2 += h.vh[k] * h.vh[k];
         const float alpha = static_cast<float>(p.alpha);
         const float vout = sqrtf(alpha * vr * vr + (1.0f - alpha) * vold2);
         const float flyd = static_cast<float>(rng.w[1]) * (kPiF / 4294967296.0f) + thi - 0.5f * kPiF;
@@ -295,7 +356,6 @@ __device__ bool launch(const FastInst &I, Reg &r, StatAcc &st, float local_T, fl
         v[2] = sf * vout;
         if (sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) >= static_cast<float>(p.ve)) return false;
     } else {
-        // flux-weighted Maxwell-Boltzmann: Rayleigh normal and Gaussian tangential components
         // the same maps of the random words as the FP64 path: log(1 - u) and angle 2 pi u
         const float sigma = sqrtf(static_cast<float>(p.kB_over_m) * local_T);
         const float vn = sigma * sqrtf(-2.0f * logf(1.0f - unit_open(rng.w[0])));
@@ -321,46 +381,24 @@ __device__ bool launch(const FastInst &I, Reg &r, StatAcc &st, float local_T, fl
         if (E < 0.0) st.bound++;
     }
     const double vd[3] = {v[0], v[1], v[2]};
-    set_vel(r, vd);
+    set_vel(h, vd);
     const double R0 = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
     const double g = p.GM / (R0 * R0 * R0);
 #pragma unroll
-    for (int k = 0; k < 3; k++) r.oa[k] = static_cast<float>(g * s[k]);
-    r.hop = 0;
+    for (int k = 0; k < 3; k++) h.oa[k] = static_cast<float>(g * s[k]);
+    h.hop = 0;
     return true;
-}
-
-
-__device__ __forceinline__ void ref_index(float thi, float fi, int ftd, int ffd, int &td, int &fd) {
-    td = static_cast<int>(ceilf((thi + 0.5f * kPiF) / kPiF * ftd)) - 1;
-    fd = static_cast<int>(ceilf(fi / (2.0f * kPiF) * ffd)) - 1;
-    td = min(max(td, 0), ftd - 1);
-    fd = min(max(fd, 0), ffd - 1);
-}
-
-__device__ __forceinline__ void angles_of(const Reg &r, float &thi, float &fi) {
-    double s[3];
-    get_pos(r, s);
-    const double R = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
-    thi = static_cast<float>(asin(s[2] / R));
-    double f = atan2(s[0], s[1]);
-    if (f < 0) f += 2.0 * kPi;
-    fi = static_cast<float>(f);
-}
-
-__device__ __forceinline__ void horizon_add(const FastInst &I, int td, int fd, float W) {
-    atomicAdd(&I.t.horizon[td * I.p.ffd + fd], __float2ull_rn(W * 16777216.0f));
 }
 
 // Start of a hop (ballistic.c:124-181, advanced.c:271-333): weight and life checks, the
 // reference freeze scan, the launch and the starting cell. Returns 0 when the particle flies,
 // else its fate.
-__device__ int hop_top(const FastInst &I, Reg &r, StatAcc &st, float &thi, float &fi,
-                       float local_T) {
+__device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h, Bounds &b,
+                       StatAcc &st, float thi, float fi, float local_T) {
     const dsmc_params &p = I.p;
-    const float W = weight(I, r);
+    const float W = weight(I, h);
     if (W < static_cast<float>(p.w_min)) return DSMC_FATE_PHOTOLYSED;
-    if (p.life_step_cap > 0 && r.steps >= p.life_step_cap) return DSMC_FATE_STEP_CAP;
+    if (p.life_step_cap > 0 && h.steps >= p.life_step_cap) return DSMC_FATE_STEP_CAP;
     if (p.model == DSMC_MODEL_REFERENCE) {
         const int ftd = p.ftd, ffd = p.ffd;
         int td, fd;
@@ -369,9 +407,10 @@ __device__ int hop_top(const FastInst &I, Reg &r, StatAcc &st, float &thi, float
         local_T = static_cast<float>(T[td * ffd + fd]);
         if (local_T < static_cast<float>(p.freeze_T)) {
             bool found = false;
+            float rest = a.s.rest[i];
             if (p.runner == DSMC_RUNNER_BALLISTIC) {
                 for (int add = 0; add < ffd; add++) {
-                    r.rest += static_cast<float>(p.dt_rot);
+                    rest += static_cast<float>(p.dt_rot);
                     const int check = (fd + add + 1) % ffd;
                     if (T[td * ffd + check] >= p.freeze_T) {
                         fd = check;
@@ -383,16 +422,16 @@ __device__ int hop_top(const FastInst &I, Reg &r, StatAcc &st, float &thi, float
             } else {
                 horizon_add(I, td, fd, W);
                 for (int add = 1; add <= ffd; add++) {
-                    r.rest += static_cast<float>(p.dt_rot);
+                    rest += static_cast<float>(p.dt_rot);
                     if (T[td * ffd + (add % ffd)] >= p.freeze_T) {
                         const double rot_fi = static_cast<double>(add - fd) / ffd * 2.0 * kPi;
                         const double cs = cos(rot_fi), sn = sin(rot_fi);
                         double s[3];
-                        get_pos(r, s);
+                        get_pos(h, s);
                         const double n0 = s[0] * cs - s[1] * sn, n1 = s[0] * sn + s[1] * cs;
                         s[0] = n0;
                         s[1] = n1;
-                        set_pos(r, s);
+                        set_pos(h, s);
                         fd = add % ffd;
                         fi = (fd + 0.5f) / ffd * 2.0f * kPiF;
                         found = true;
@@ -400,6 +439,7 @@ __device__ int hop_top(const FastInst &I, Reg &r, StatAcc &st, float &thi, float
                     }
                 }
             }
+            a.s.rest[i] = rest;
             if (!found) {
                 horizon_add(I, td, fd, W);
                 return DSMC_FATE_FROZEN;
@@ -407,83 +447,88 @@ __device__ int hop_top(const FastInst &I, Reg &r, StatAcc &st, float &thi, float
             local_T = static_cast<float>(T[td * ffd + fd]);
         }
     }
-    if (!launch(I, r, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
-    int ht, td, fd;
-    cell_from_scratch(I, r.sh[0] + r.sl[0], r.sh[1] + r.sl[1], r.sh[2] + r.sl[2], ht, td, fd);
-    r.cell = pack_cell(ht, td, fd);
+    if (!launch(a, i, I, h, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
+    enter_cell(I, h, b, cell_from_scratch(I, h.sh[0] + h.sl[0], h.sh[1] + h.sl[1], h.sh[2] + h.sl[2]));
     return 0;
 }
 
 // Landing (ballistic.c:239-264): polar deposit (reference) or night freeze-out / day-side
 // re-emission point (config). Returns 0 to start a new hop, else the fate.
-__device__ int land(const FastInst &I, Reg &r, float &thi, float &fi, float &local_T) {
+__device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &local_T) {
     const dsmc_params &p = I.p;
-    angles_of(r, thi, fi);
+    angles_of(h, thi, fi);
     int td, fd;
     ref_index(thi, fi, p.ftd, p.ffd, td, fd);
     if (p.model == DSMC_MODEL_REFERENCE) {
         if (td <= 1 || td >= p.ftd - 2) {
-            horizon_add(I, td, fd, 0.05f * weight(I, r));
-            r.w0 *= 0.95f;
+            horizon_add(I, td, fd, 0.05f * weight(I, h));
+            h.w0 *= 0.95f;
         }
         return 0;
     }
     double s[3];
-    get_pos(r, s);
+    get_pos(h, s);
     const double R = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
     double n[3] = {s[0] / R, s[1] / R, s[2] / R};
     if (n[0] * p.sun[0] + n[1] * p.sun[1] + n[2] * p.sun[2] <= 0.0) {
-        horizon_add(I, td, fd, weight(I, r));
+        horizon_add(I, td, fd, weight(I, h));
         return DSMC_FATE_FROZEN;
     }
     for (int k = 0; k < 3; k++) s[k] = n[k] * p.Radii;
-    set_pos(r, s);
+    set_pos(h, s);
     local_T = static_cast<float>(I.t.face_T[locate_face(I.t, n)]);
     return 0;
 }
 
-// End of a particle's life: per-particle rows, counters, deposit runs flushed.
-__device__ void finish(const FastInst &I, Reg &r, StatAcc &st, int fate) {
+// End of a particle's life: per-particle rows (layout of ballistic.c:120,273-276 and
+// advanced.c:262-267,439-444), counters, deposits flushed.
+__device__ void finish(const FastArgs &a, long long i, const FastInst &I, Hot &h, StatAcc &st,
+                       int fate) {
     const dsmc_params &p = I.p;
     const DevTables &t = I.t;
     const bool ref = p.model == DSMC_MODEL_REFERENCE, adv = p.runner == DSMC_RUNNER_ADVANCED;
-    const long long slot = static_cast<long long>(r.pid) - t.out_base;
+    const unsigned pid = a.s.pid[i];
+    const int ncol = a.s.ncol[i];
+    const long long slot = static_cast<long long>(pid) - t.out_base;
     if (slot >= 0 && slot < t.out_cap) {
         if (t.ttime && (fate != DSMC_FATE_ESCAPED || !ref)) {
             float thi, fi;
-            angles_of(r, thi, fi);
-            const double flight = static_cast<double>(r.steps) * p.dt_step;
+            angles_of(h, thi, fi);
+            const float rest = a.s.rest[i];
+            const double flight = static_cast<double>(h.steps) * p.dt_step;
             t.ttime[1 * t.out_cap + slot] = thi;
-            t.ttime[2 * t.out_cap + slot] = flight + r.rest;
-            t.ttime[3 * t.out_cap + slot] = weight(I, r);
+            t.ttime[2 * t.out_cap + slot] = flight + rest;
+            t.ttime[3 * t.out_cap + slot] = weight(I, h);
             t.ttime[4 * t.out_cap + slot] = flight;
             if (adv || !ref) {
-                t.ttime[7 * t.out_cap + slot] = r.rest;
-                t.ttime[8 * t.out_cap + slot] = r.ncol;
+                t.ttime[7 * t.out_cap + slot] = rest;
+                t.ttime[8 * t.out_cap + slot] = ncol;
             }
         }
         if (t.fate) t.fate[slot] = fate;
-        if (t.steps) t.steps[slot] = r.steps;
+        if (t.steps) t.steps[slot] = h.steps;
     }
     st.finished++;
-    st.collisions += r.ncol;
+    st.collisions += ncol;
     if (fate == DSMC_FATE_ESCAPED) st.escaped++;
-    flush_run(I, r);
-    r.inst = -1;
+    flush_cell(I, h);
+    flush_hist(I, h);
+    h.ci = -1;
+    h.inst = -1;
 }
 
 // A collision against a partner drawn from the cell's fitted speed CDF (advanced.c:374-396).
-__device__ void collide(const FastInst &I, Reg &r, long long pidx) {
+__device__ void collide(const FastArgs &a, long long i, const FastInst &I, Hot &h, long long pidx) {
     const dsmc_params &p = I.p;
     const DevTables &t = I.t;
     Philox rng;
-    rng.init(p.seed, p.instance, r.pid);
-    rng.event = r.evt;
+    rng.init(p.seed, p.instance, a.s.pid[i]);
+    rng.event = a.s.evt[i];
     rng.next();
     const double *coef = t.cdf_coef + DSMC_CDF_STRIDE * pidx;
     const double *box = t.cdf_box + 4 * pidx;
     double v[3];
-    get_vel(r, v);
+    get_vel(h, v);
     const double vv2 = cdf_sample(coef, box, t.cdf_total[pidx], t.cdf_degree, rng.raw(0) / kTwo32);
     double col_p = -1.0;
     if (p.scatter == DSMC_SCATTER_REFERENCE) {
@@ -507,11 +552,11 @@ __device__ void collide(const FastInst &I, Reg &r, long long pidx) {
         const double hg = 0.5 * sqrt(g2);
         for (int k = 0; k < 3; k++) v[k] = vcm[k] + hg * om[k];
     }
-    r.evt = rng.event;
-    if (col_p >= 0.0) r.pthr = static_cast<float>(-log1p(-col_p));
-    set_vel(r, v);
-    r.pcol = 0.0f;
-    r.ncol++;
+    a.s.evt[i] = rng.event;
+    a.s.ncol[i] += 1;
+    if (col_p >= 0.0) h.pthr = static_cast<float>(-log1p(-col_p));
+    set_vel(h, v);
+    h.pcol = 0.0f;
 }
 
 // Next work index of the device queue: one atomic per group of lanes asking together.
@@ -538,7 +583,7 @@ __device__ __forceinline__ int find_inst(const FastArgs &a, unsigned long long w
 // Fill an empty slot with the next particle from the queue and launch it; particles that end
 // at their first launch are finished here and the next one is taken. Returns false when the
 // queue is empty.
-__device__ bool start_next(const FastArgs &a, Reg &r, StatAcc &st) {
+__device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, StatAcc &st) {
     for (;;) {
         const unsigned long long w = grab_work(a.ctr);
         if (w >= static_cast<unsigned long long>(a.total)) return false;
@@ -546,37 +591,25 @@ __device__ bool start_next(const FastArgs &a, Reg &r, StatAcc &st) {
         const FastInst &I = a.inst[ii];
         const dsmc_params &p = I.p;
         if (ii != st.inst) {
-            // counters belong to one instance: add the previous instance's share lane by lane
-            if (st.inst >= 0) {
-                unsigned long long *dst = a.inst[st.inst].t.stats;
-                if (st.steps) atomicAdd(dst + kStatSteps, static_cast<unsigned long long>(st.steps));
-                if (st.escaped) atomicAdd(dst + kStatEscaped, static_cast<unsigned long long>(st.escaped));
-                if (st.collisions) atomicAdd(dst + kStatCollisions, static_cast<unsigned long long>(st.collisions));
-                if (st.bound) atomicAdd(dst + kStatBound, static_cast<unsigned long long>(st.bound));
-                if (st.finished) atomicAdd(dst + kStatFinished, static_cast<unsigned long long>(st.finished));
-                if (st.finished) atomicAdd(&a.ctr->finished, static_cast<unsigned long long>(st.finished));
-            }
-            st = StatAcc{};
+            flush_stats_lane(a, st);
             st.inst = ii;
         }
-        r.inst = ii;
-        r.pid = static_cast<unsigned>(I.pid_begin + static_cast<long long>(w - I.work_base));
+        const unsigned pid = static_cast<unsigned>(I.pid_begin + static_cast<long long>(w - I.work_base));
+        h.inst = ii;
         Philox rng;
-        rng.init(p.seed, p.instance, r.pid);
+        rng.init(p.seed, p.instance, pid);
         rng.next();
-        r.w0 = 1.0f;
-        r.nday = 0;
-        r.steps = 0;
-        r.hop = 0;
-        r.pcol = 0.0f;
-        r.ncol = 0;
-        r.rest = 0.0f;
-        r.run_cell = -1;
-        r.run_acc = 0;
-        r.hist_key = -1;
-        r.hist_cnt = 0;
+        h.w0 = 1.0f;
+        h.nday = 0;
+        h.steps = 0;
+        h.hop = 0;
+        h.pcol = 0.0f;
+        h.ci = -1;
+        h.acc = 0;
+        h.hist_key = -1;
+        h.hist_cnt = 0;
         const double zero[3] = {0.0, 0.0, 0.0};
-        set_vel(r, zero);
+        set_vel(h, zero);
         float thi, fi, local_T = 0.0f;
         double col_p = 0.0;
         double s[3];
@@ -606,12 +639,14 @@ __device__ bool start_next(const FastArgs &a, Reg &r, StatAcc &st) {
             for (int k = 0; k < 3; k++) s[k] = q[k] * (p.Radii / lq);
             local_T = static_cast<float>(I.t.face_T[f]);
         }
-        r.evt = rng.event;
-        r.pthr = static_cast<float>(-log1p(-col_p));
-        set_pos(r, s);
-        if (p.model != DSMC_MODEL_REFERENCE) angles_of(r, thi, fi);
-        r.thi0 = thi;
-        const long long slot = static_cast<long long>(r.pid) - I.t.out_base;
+        a.s.pid[i] = pid;
+        a.s.evt[i] = rng.event;
+        a.s.ncol[i] = 0;
+        a.s.rest[i] = 0.0f;
+        h.pthr = static_cast<float>(-log1p(-col_p));
+        set_pos(h, s);
+        if (p.model != DSMC_MODEL_REFERENCE) angles_of(h, thi, fi);
+        const long long slot = static_cast<long long>(pid) - I.t.out_base;
         if (I.t.ttime && slot >= 0 && slot < I.t.out_cap) {
             I.t.ttime[slot] = thi;
             if (p.runner == DSMC_RUNNER_ADVANCED || p.model != DSMC_MODEL_REFERENCE) {
@@ -619,152 +654,165 @@ __device__ bool start_next(const FastArgs &a, Reg &r, StatAcc &st) {
                 I.t.ttime[6 * I.t.out_cap + slot] = local_T;
             }
         }
-        const int fate = hop_top(I, r, st, thi, fi, local_T);
+        const int fate = hop_top(a, i, I, h, b, st, thi, fi, local_T);
         if (fate == 0) return true;
-        finish(I, r, st, fate);
+        finish(a, i, I, h, st, fate);
     }
 }
 
 // One Verlet step of the reference's variant with (hi, lo) position and velocity sums.
 // (x, y, z, r2) hold the current position on entry and the new one on exit; d the displacement.
-__device__ __forceinline__ void verlet_f32(Reg &r, float &x, float &y, float &z, float &r2,
-                                           float GM, float h, float c1, float c2, float d[3]) {
+__device__ __forceinline__ void verlet_f32(Hot &h, float &x, float &y, float &z, float &r2,
+                                           float GM, float dt, float c1, float c2, float d[3]) {
     const float ir = rsqrtf(r2);
     const float g = GM * (ir * ir * ir);
-    const float a[3] = {g * x, g * y, g * z};
+    const float acc[3] = {g * x, g * y, g * z};
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        d[k] = fmaf(r.vh[k], h, fmaf(r.vl[k], h, -fmaf(a[k], c1, r.oa[k] * c2)));
+        d[k] = fmaf(h.vh[k], dt, fmaf(h.vl[k], dt, -fmaf(acc[k], c1, h.oa[k] * c2)));
         float t, e;
-        two_sum(r.sh[k], d[k], t, e);
-        r.sh[k] = t;
-        r.sl[k] += e;
-        two_sum(r.vh[k], -a[k] * h, t, e);
-        r.vh[k] = t;
-        r.vl[k] += e;
-        r.oa[k] = a[k];
+        two_sum(h.sh[k], d[k], t, e);
+        h.sh[k] = t;
+        h.sl[k] += e;
+        two_sum(h.vh[k], -acc[k] * dt, t, e);
+        h.vh[k] = t;
+        h.vl[k] += e;
+        h.oa[k] = acc[k];
     }
-    x = r.sh[0] + r.sl[0];
-    y = r.sh[1] + r.sl[1];
-    z = r.sh[2] + r.sl[2];
+    x = h.sh[0] + h.sl[0];
+    y = h.sh[1] + h.sl[1];
+    z = h.sh[2] + h.sl[2];
     r2 = fmaf(x, x, fmaf(y, y, z * z));
 }
 
-__global__ void __launch_bounds__(256, 2) fast_kernel(const FastArgs a) {
+enum Flag { kRef = 1, kSkipFirst = 2, kCollide = 4, kHist = 8 };
+
+// kMinBlocks: resident 256-thread blocks per SM the register allocation must allow (2: up to
+// 128 registers a thread; 3: up to 80). The launch shape's blocks_per_sm picks the variant.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a) {
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    Reg r;
-    load_slot(a.s, i, a.nslots, r);
+    Hot h;
+    load_hot(a.s, i, a.nslots, h);
     StatAcc st;
-    st.inst = r.inst;
-    int budget = a.K;
-    bool alive = r.inst >= 0;
-    if (!alive) alive = start_next(a, r, st);
-    // constants of the current particle's instance
-    int cur = -1;
-    float GM = 0.f, h = 0.f, c1 = 0.f, c2 = 0.f, rl2 = 0.f, re2 = 0.f, cday = 0.f, sun0 = 0.f,
-          sun1 = 0.f, sun2 = 0.f, sig = 0.f, inv_bw = 0.f, wmin = 0.f;
-    int ftd = 0, ffd = 0, hd = 0, nbins = 0, col_ht = 0;
-    bool ref = false, skip_first = false, collide_on = false, hist_on = false;
-    long long life_cap = 0, hop_cap = 0;
+    st.inst = h.inst;
+    Bounds b;
+    bool alive = h.inst >= 0;
+    if (alive) {
+        // reload the cached bounds of the saved cell without flushing its pending deposits
+        const int ci = h.ci;
+        const unsigned long long acc = h.acc;
+        h.ci = -1;
+        enter_cell(a.inst[h.inst], h, b, h.cell);
+        h.ci = ci;
+        h.acc = acc;
+    } else {
+        alive = start_next(a, i, h, b, st);
+    }
+    int cur = -1, flags = 0, half_ffd = 0, life_cap = 0, hop_cap = 0, col_ht = 0, nbins = 0;
+    float GM = 0.f, dt = 0.f, c1 = 0.f, c2 = 0.f, rl2 = 0.f, re2 = 0.f, cday = 0.f, sx = 0.f,
+          sy = 0.f, sz = 0.f, inv_bw = 0.f;
     const FastInst *I = nullptr;
     float x = 0.f, y = 0.f, z = 0.f, r2 = 0.f;
     bool fresh = true;
+    int budget = a.K;
 
     while (alive && budget > 0) {
-        if (r.inst != cur) {
-            cur = r.inst;
+        if (h.inst != cur) {
+            cur = h.inst;
             I = &a.inst[cur];
             const dsmc_params &p = I->p;
             GM = static_cast<float>(p.GM);
-            h = static_cast<float>(p.dt_step);
+            dt = static_cast<float>(p.dt_step);
             c1 = static_cast<float>(1.5 * p.dt_step * p.dt_step);
             c2 = static_cast<float>(p.dt_step * p.dt_step / 6.0);
             rl2 = I->r_land2;
             re2 = I->r_esc2;
             cday = I->c_day;
-            sun0 = static_cast<float>(p.sun[0]);
-            sun1 = static_cast<float>(p.sun[1]);
-            sun2 = static_cast<float>(p.sun[2]);
-            ftd = p.ftd; ffd = p.ffd; hd = p.hd;
-            ref = p.model == DSMC_MODEL_REFERENCE;
-            skip_first = p.skip_first_deposit != 0;
-            collide_on = p.runner == DSMC_RUNNER_ADVANCED && I->t.n_bg != nullptr;
+            sx = static_cast<float>(p.sun[0]);
+            sy = static_cast<float>(p.sun[1]);
+            sz = static_cast<float>(p.sun[2]);
+            half_ffd = p.ffd / 2;
+            flags = (p.model == DSMC_MODEL_REFERENCE ? kRef : 0) |
+                    (p.skip_first_deposit ? kSkipFirst : 0) |
+                    (p.runner == DSMC_RUNNER_ADVANCED && I->t.n_bg ? kCollide : 0) |
+                    (I->t.speed_hist && p.n_speed_bins > 0 ? kHist : 0);
+            life_cap = p.life_step_cap > 0
+                           ? static_cast<int>(min(static_cast<long long>(p.life_step_cap), 0x7fffffffLL))
+                           : 0x7fffffff;
+            hop_cap = static_cast<int>(min(static_cast<long long>(p.hop_step_cap), 0x7fffffffLL));
             col_ht = p.collide_ht_max;
-            sig = static_cast<float>(p.cross_section);
-            hist_on = I->t.speed_hist != nullptr && p.n_speed_bins > 0;
             nbins = p.n_speed_bins;
-            inv_bw = hist_on ? static_cast<float>(1.0 / p.speed_bin_width) : 0.f;
-            life_cap = p.life_step_cap;
-            hop_cap = p.hop_step_cap;
-            wmin = static_cast<float>(p.w_min);
+            inv_bw = nbins > 0 ? static_cast<float>(1.0 / p.speed_bin_width) : 0.f;
         }
         if (fresh) {
-            x = r.sh[0] + r.sl[0];
-            y = r.sh[1] + r.sl[1];
-            z = r.sh[2] + r.sl[2];
+            x = h.sh[0] + h.sl[0];
+            y = h.sh[1] + h.sl[1];
+            z = h.sh[2] + h.sl[2];
             r2 = fmaf(x, x, fmaf(y, y, z * z));
             fresh = false;
         }
         float d[3];
-        verlet_f32(r, x, y, z, r2, GM, h, c1, c2, d);
+        verlet_f32(h, x, y, z, r2, GM, dt, c1, c2, d);
         budget--;
-        const int ii = r.hop;
-        r.steps++;
-        r.hop++;
+        const int ii = h.hop;
+        h.steps++;
+        h.hop++;
+        st.steps++;
         int event = 0;   // 1 landed (or hop cap), 2 escaped, 3 life cap
-        if (r2 <= rl2) {
-            event = 1;
-        } else if (r2 >= re2) {
-            event = 2;
-        } else {
-            int ht = r.cell >> 16, td = (r.cell >> 8) & 0xff, fd = r.cell & 0xff;
-            track_shell(*I, r2, ht);
-            track_angles(*I, x, y, z, r2, td, fd);
-            r.cell = pack_cell(ht, td, fd);
-            const bool day = ref ? (fd < ffd / 2) : (fmaf(x, sun0, fmaf(y, sun1, z * sun2)) > 0.0f);
-            if (day) r.nday++;
-            if (!(skip_first && ii == 0)) {
-                const int ci = (ht * ftd + td) * ffd + fd;
+        const float zz = z * fabsf(z);
+        const bool inside = (r2 > b.r2lo) & (r2 <= b.r2hi) & (zz > r2 * b.zlo) &
+                            (zz <= r2 * b.zhi) & (x * b.c0 - y * b.s0 > 0.0f) &
+                            (x * b.c1 - y * b.s1 <= 0.0f);
+        if (!inside) {
+            if (r2 <= rl2) {
+                event = 1;
+            } else if (r2 >= re2) {
+                event = 2;
+            } else {
+                int ht = h.cell >> 16, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
+                track_shell(*I, r2, ht);
+                track_angles(*I, x, y, z, r2, td, fd);
+                const int cell = pack_cell(ht, td, fd);
+                if (cell != h.cell) enter_cell(*I, h, b, cell);
+            }
+        }
+        if (!event) {
+            const bool day = (flags & kRef) ? ((h.cell & 0xff) < half_ffd)
+                                            : (fmaf(x, sx, fmaf(y, sy, z * sz)) > 0.0f);
+            h.nday += day;
+            if (!((flags & kSkipFirst) && ii == 0)) {
                 bool collided = false;
-                if (collide_on && ht < col_ht) {
-                    const float nb = ci < I->t.n_bg_len ? static_cast<float>(__ldg(I->t.n_bg + ci)) : 0.f;
-                    r.pcol += sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) * nb * sig;
-                    if (r.pcol > r.pthr) {
-                        const long long pidx = (static_cast<long long>(td) * ffd + fd) * hd + ht;
-                        if (__ldg(I->t.cdf_valid + pidx)) {
-                            collide(*I, r, pidx);
+                if ((flags & kCollide) && h.nsig > 0.0f) {
+                    h.pcol = fmaf(sqrtf(fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2]))), h.nsig, h.pcol);
+                    if (h.pcol > h.pthr) {
+                        const int ht = h.cell >> 16, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
+                        const long long pidx = (static_cast<long long>(td) * I->p.ffd + fd) * I->p.hd + ht;
+                        if (ht < col_ht && __ldg(I->t.cdf_valid + pidx)) {
+                            collide(a, i, *I, h, pidx);
                             collided = true;
                         }
                     }
                 }
                 if (!collided) {
-                    const float W = r.w0 * exp2f(-cday * static_cast<float>(r.nday));
-                    const unsigned long long q = __float2ull_rn(W * 16777216.0f);
-                    if (ci == r.run_cell) {
-                        r.run_acc += q;
-                    } else {
-                        if (r.run_cell >= 0) atomicAdd(&I->t.density[r.run_cell], r.run_acc);
-                        r.run_cell = ci;
-                        r.run_acc = q;
-                    }
-                    if (hist_on) {
-                        const float sp = sqrtf(fmaf(r.vh[0], r.vh[0], fmaf(r.vh[1], r.vh[1], r.vh[2] * r.vh[2])));
-                        const int b = min(static_cast<int>(sp * inv_bw), nbins - 1);
-                        const int key = ci * nbins + b;
-                        if (key == r.hist_key) {
-                            r.hist_cnt++;
+                    const float W = h.w0 * exp2f(-cday * static_cast<float>(h.nday));
+                    h.acc += __float2uint_rn(W * 16777216.0f);
+                    if (flags & kHist) {
+                        const float sp = sqrtf(fmaf(h.vh[0], h.vh[0], fmaf(h.vh[1], h.vh[1], h.vh[2] * h.vh[2])));
+                        const int key = h.ci * nbins + min(static_cast<int>(sp * inv_bw), nbins - 1);
+                        if (key == h.hist_key) {
+                            h.hist_cnt++;
                         } else {
-                            if (r.hist_key >= 0) atomicAdd(&I->t.speed_hist[r.hist_key], static_cast<unsigned long long>(r.hist_cnt));
-                            r.hist_key = key;
-                            r.hist_cnt = 1;
+                            flush_hist(*I, h);
+                            h.hist_key = key;
+                            h.hist_cnt = 1;
                         }
                     }
                 }
             }
-            if (life_cap > 0 && r.steps >= life_cap) event = 3;
-            else if (r.hop >= hop_cap) event = 1;
+            if (h.steps >= life_cap) event = 3;
+            else if (h.hop >= hop_cap) event = 1;
         }
-        st.steps++;
         if (event) {
             fresh = true;
             int fate = 0;
@@ -774,25 +822,20 @@ __global__ void __launch_bounds__(256, 2) fast_kernel(const FastArgs a) {
                 fate = DSMC_FATE_STEP_CAP;
             } else {
                 float thi, fi, local_T = 0.f;
-                fate = land(*I, r, thi, fi, local_T);
-                if (fate == 0) fate = hop_top(*I, r, st, thi, fi, local_T);
+                fate = land(*I, h, thi, fi, local_T);
+                if (fate == 0) fate = hop_top(a, i, *I, h, b, st, thi, fi, local_T);
             }
             if (fate) {
-                finish(*I, r, st, fate);
-                alive = start_next(a, r, st);
+                finish(a, i, *I, h, st, fate);
+                alive = start_next(a, i, h, b, st);
             }
         }
-        (void)wmin;
     }
-    if (!alive && r.inst >= 0) {
-        // (not reached: a slot without a particle has inst = -1)
-    }
-    store_slot(a.s, i, a.nslots, r);
+    store_hot(a.s, i, a.nslots, h);
     // statistics of this launch, per instance; the finished count also drives the host loop
     const unsigned fin = st.finished;
     flush_stats(a, st);
-    const unsigned full = 0xffffffffu;
-    const unsigned wfin = __reduce_add_sync(full, fin);
+    const unsigned wfin = __reduce_add_sync(0xffffffffu, fin);
     if ((threadIdx.x & 31) == 0 && wfin) atomicAdd(&a.ctr->finished, static_cast<unsigned long long>(wfin));
 }
 
@@ -801,30 +844,30 @@ __global__ void push_fp32_kernel(const dsmc_params p, long long n, int nsteps, d
                                  double *vel, int *status, int *taken) {
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    Reg r;
+    Hot h;
     const double s[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
     const double v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
-    set_pos(r, s);
-    set_vel(r, v);
+    set_pos(h, s);
+    set_vel(h, v);
     const double R0 = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
     const double g0 = p.GM / (R0 * R0 * R0);
-    for (int k = 0; k < 3; k++) r.oa[k] = static_cast<float>(g0 * s[k]);
-    const float GM = static_cast<float>(p.GM), h = static_cast<float>(p.dt_step);
+    for (int k = 0; k < 3; k++) h.oa[k] = static_cast<float>(g0 * s[k]);
+    const float GM = static_cast<float>(p.GM), dt = static_cast<float>(p.dt_step);
     const float c1 = static_cast<float>(1.5 * p.dt_step * p.dt_step);
     const float c2 = static_cast<float>(p.dt_step * p.dt_step / 6.0);
     const float rl2 = static_cast<float>(p.Radii * p.Radii);
     const float re2 = static_cast<float>(p.max_height * p.max_height);
-    float x = r.sh[0] + r.sl[0], y = r.sh[1] + r.sl[1], z = r.sh[2] + r.sl[2];
+    float x = h.sh[0] + h.sl[0], y = h.sh[1] + h.sl[1], z = h.sh[2] + h.sl[2];
     float r2 = fmaf(x, x, fmaf(y, y, z * z));
     int st = 0, k = 0;
     for (; k < nsteps && st == 0; k++) {
         float d[3];
-        verlet_f32(r, x, y, z, r2, GM, h, c1, c2, d);
+        verlet_f32(h, x, y, z, r2, GM, dt, c1, c2, d);
         st = r2 <= rl2 ? 1 : (r2 >= re2 ? 2 : 0);
     }
     double so[3], vo[3];
-    get_pos(r, so);
-    get_vel(r, vo);
+    get_pos(h, so);
+    get_vel(h, vo);
     for (int j = 0; j < 3; j++) { pos[3 * i + j] = so[j]; vel[3 * i + j] = vo[j]; }
     status[i] = st;
     taken[i] = k;
@@ -861,10 +904,20 @@ void FastEngine::free_all() {
     nslots_ = 0;
 }
 
+namespace {
+
+// The two register budgets of fast_kernel (see kMinBlocks).
+void (*kernel_variant(int variant))(FastArgs) {
+    return variant >= 3 ? fast_kernel<3> : fast_kernel<2>;
+}
+
+}  // namespace
+
 cudaError_t FastEngine::ensure_slots(int num_sms) {
     // one wave: as many blocks per SM as can be resident together
+    variant_ = blocks_per_sm >= 3 ? 3 : 2;
     int resident = 0;
-    cudaError_t e0 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fast_kernel, block, 0);
+    cudaError_t e0 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel_variant(variant_), block, 0);
     if (e0 != cudaSuccess) return e0;
     if (resident < 1) return cudaErrorInvalidConfiguration;
     const int per_sm = (blocks_per_sm > resident || blocks_per_sm < 1) ? resident : blocks_per_sm;
@@ -1016,14 +1069,14 @@ cudaError_t FastEngine::drain(long long total, cudaStream_t stream) {
     a.total = total;
     a.K = steps_per_launch;
     const unsigned grid = static_cast<unsigned>(nslots_ / block);
-    const int key[4] = {static_cast<int>(total & 0x7fffffff), static_cast<int>(total >> 31), ninst_,
-                        steps_per_launch * 64 + launches_per_graph};
+    const int key[4] = {static_cast<int>(total & 0x7fffffff), static_cast<int>(total >> 31),
+                        ninst_ * 8 + variant_, steps_per_launch * 64 + launches_per_graph};
     const bool use_graph = launches_per_graph > 1;
     if (use_graph && (!graph_ || graph_stream_ != stream || std::memcmp(key, graph_key_, sizeof key) != 0)) {
         if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
         cudaGraph_t g;
         if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-        for (int k = 0; k < launches_per_graph; k++) fast_kernel<<<grid, block, 0, stream>>>(a);
+        for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_)<<<grid, block, 0, stream>>>(a);
         if ((e = cudaStreamEndCapture(stream, &g)) != cudaSuccess) return e;
         e = cudaGraphInstantiate(&graph_, g, 0);
         cudaGraphDestroy(g);
@@ -1042,7 +1095,7 @@ cudaError_t FastEngine::drain(long long total, cudaStream_t stream) {
             if ((e = cudaGraphLaunch(graph_, stream)) != cudaSuccess) return e;
             launches += launches_per_graph;
         } else {
-            fast_kernel<<<grid, block, 0, stream>>>(a);
+            kernel_variant(variant_)<<<grid, block, 0, stream>>>(a);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             launches += 1;
         }

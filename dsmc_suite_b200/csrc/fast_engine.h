@@ -106,6 +106,7 @@ private:
     cudaStream_t graph_stream_ = nullptr;
     int graph_key_[4] = {0, 0, 0, 0};
     bool nslots_want_changed_ = false;
+    int variant_ = 2;
 };
 
 }  // namespace dsmc
