@@ -140,6 +140,9 @@ SIGNATURES = [
     ("dsmc_push_host", C.c_int, [_P, C.c_int, C.c_int64, C.c_int, _DP, _DP, _I32P, _I32P]),
     ("dsmc_velocity_record", C.c_int, [_P, C.c_int64, C.c_int, C.c_int64, _DP, _I32P, _I32P, _I32P,
                                        _I64P]),
+    ("dsmc_solve_fast_noalloc", C.c_int, [C.POINTER(Params), C.POINTER(Surface), C.c_int64,
+                                          C.c_int64, _U64P, _U64P, _U64P, _P]),
+    ("dsmc_noalloc_last_error", C.c_char_p, []),
     ("dsmc_solve_host", C.c_int, [_P, C.c_int, C.POINTER(Params), C.POINTER(Surface),
                                   C.POINTER(Collision), C.c_int64, _U64P, _U64P, C.POINTER(Stats)]),
 ]

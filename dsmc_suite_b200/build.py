@@ -36,6 +36,7 @@ CUDA_SOURCES = {
     "kernel_fit.cu": ["-fmad=false"],
     "fast_engine.cu": [],
     "kernel_peak.cu": [],
+    "noalloc.cu": [],
     "dsmc_abi.cu": [],
 }
 C_SOURCES = ["host_setup.c", "host_scalar.c", "host_fileio.c", "host_runners.c"]

@@ -1133,4 +1133,116 @@ cudaError_t FastEngine::run_batch(const std::vector<dsmc_params> &ps, const std:
     return drain(total, stream);
 }
 
+size_t fast_slot_bytes(long long nslots) {
+    return static_cast<size_t>(nslots) * (31 * 4 + 8) + 256;
+}
+
+size_t fast_inst_bytes() { return sizeof(FastInst); }
+
+size_t fast_counter_bytes() { return sizeof(FastCounters); }
+
+cudaError_t fast_fill_instance(const dsmc_params &p, const DevTables &t, long long pid_begin,
+                               long long n, float *d_tab, size_t tab_floats, void *inst_host,
+                               float *tab_host) {
+    const size_t need = static_cast<size_t>(p.hd + 1) + (p.ftd + 1) + 1 + 2 * (p.ffd + 1);
+    if (need > tab_floats) return cudaErrorInvalidValue;
+    float *rb2 = tab_host, *sbs = rb2 + (p.hd + 1);
+    size_t lo = static_cast<size_t>(p.hd + 1) + (p.ftd + 1);
+    lo = (lo + 1) & ~static_cast<size_t>(1);
+    float *lon = tab_host + lo;
+    for (int j = 0; j <= p.hd; j++) {
+        const double rj = p.use_exp_grid ? p.Radii + p.unih * (std::pow(1.0 + p.alpha2, j) - 1.0) / p.alpha2
+                                         : p.Radii + j * p.unih;
+        rb2[j] = static_cast<float>(rj * rj);
+    }
+    for (int j = 0; j <= p.ftd; j++) {
+        const double sb = std::sin(static_cast<double>(j) / p.ftd * kPi - kPi / 2.0);
+        sbs[j] = static_cast<float>(sb * std::fabs(sb));
+    }
+    sbs[0] = -1.0f;
+    sbs[p.ftd] = 1.0f;
+    for (int j = 0; j <= p.ffd; j++) {
+        const double ph = 2.0 * kPi * j / p.ffd;
+        lon[2 * j] = static_cast<float>(std::sin(ph));
+        lon[2 * j + 1] = static_cast<float>(std::cos(ph));
+    }
+    lon[0] = 0.0f; lon[1] = 1.0f;
+    lon[2 * p.ffd] = 0.0f; lon[2 * p.ffd + 1] = 1.0f;
+    FastInst &I = *static_cast<FastInst *>(inst_host);
+    std::memset(&I, 0, sizeof I);
+    I.p = p;
+    I.t = t;
+    I.rb2 = d_tab;
+    I.sbs = d_tab + (p.hd + 1);
+    I.lonb = reinterpret_cast<const float2 *>(d_tab + lo);
+    I.work_base = 0;
+    I.n = n;
+    I.pid_begin = pid_begin;
+    I.c_day = static_cast<float>(p.dt_step / p.lifetime / std::log(2.0));
+    I.r_land2 = static_cast<float>(p.Radii * p.Radii);
+    I.r_esc2 = static_cast<float>(p.max_height * p.max_height);
+    return cudaSuccess;
+}
+
+cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long nslots, void *d_ctr,
+                                long long total, int steps_per_launch, int block,
+                                cudaStream_t stream, long long *launches) {
+    *launches = 0;
+    if (total <= 0) return cudaSuccess;
+    if (nslots % block) return cudaErrorInvalidValue;
+    const long long S = nslots;
+    char *b = static_cast<char *>(slot_mem);
+    auto take = [&](size_t each) { char *q = b; b += static_cast<size_t>(S) * each; return q; };
+    Slots s{};
+    s.run_acc = reinterpret_cast<unsigned long long *>(take(8));
+    s.inst = reinterpret_cast<int *>(take(4));
+    s.pid = reinterpret_cast<unsigned *>(take(4));
+    s.evt = reinterpret_cast<unsigned *>(take(4));
+    s.sh = reinterpret_cast<float *>(take(12));
+    s.sl = reinterpret_cast<float *>(take(12));
+    s.vh = reinterpret_cast<float *>(take(12));
+    s.vl = reinterpret_cast<float *>(take(12));
+    s.oa = reinterpret_cast<float *>(take(12));
+    s.w0 = reinterpret_cast<float *>(take(4));
+    s.nday = reinterpret_cast<int *>(take(4));
+    s.steps = reinterpret_cast<int *>(take(4));
+    s.hop = reinterpret_cast<int *>(take(4));
+    s.cell = reinterpret_cast<int *>(take(4));
+    s.run_cell = reinterpret_cast<int *>(take(4));
+    s.hist_key = reinterpret_cast<int *>(take(4));
+    s.hist_cnt = reinterpret_cast<int *>(take(4));
+    s.pcol = reinterpret_cast<float *>(take(4));
+    s.pthr = reinterpret_cast<float *>(take(4));
+    s.ncol = reinterpret_cast<int *>(take(4));
+    s.rest = reinterpret_cast<float *>(take(4));
+    s.thi0 = reinterpret_cast<float *>(take(4));
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(d_ctr, 0, sizeof(FastCounters), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(s.inst, 0xff, S * sizeof(int), stream)) != cudaSuccess) return e;
+    FastArgs a{};
+    a.inst = static_cast<const FastInst *>(d_inst);
+    a.ninst = 1;
+    a.s = s;
+    a.nslots = S;
+    a.ctr = static_cast<FastCounters *>(d_ctr);
+    a.total = total;
+    a.K = steps_per_launch;
+    const unsigned grid = static_cast<unsigned>(S / block);
+    FastCounters host{};
+    unsigned long long last = 0;
+    long long stalled = 0;
+    for (;;) {
+        if (stalled > 4096) return cudaErrorLaunchTimeout;
+        fast_kernel<2><<<grid, block, 0, stream>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        *launches += 1;
+        if ((e = cudaMemcpyAsync(&host, d_ctr, sizeof host, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+        if (host.finished >= static_cast<unsigned long long>(total)) return cudaSuccess;
+        stalled = host.finished == last ? stalled + 1 : 0;
+        last = host.finished;
+    }
+}
+
 }  // namespace dsmc

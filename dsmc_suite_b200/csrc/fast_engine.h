@@ -52,6 +52,21 @@ struct FastCounters {
     unsigned long long finished;  // particles whose life ended
 };
 
+// Pieces of the engine for callers that supply every buffer themselves (no allocation here):
+// bytes of the slot arrays for nslots slots, of one instance descriptor and of the counters;
+// fast_fill_instance builds one descriptor and its boundary tables in host memory (tab_host,
+// tab_floats entries; d_tab is where the caller will copy them); fast_drain_external runs the
+// launch loop without graphs on caller memory until the queue of `total` particles is empty.
+size_t fast_slot_bytes(long long nslots);
+size_t fast_inst_bytes();
+size_t fast_counter_bytes();
+cudaError_t fast_fill_instance(const dsmc_params &p, const DevTables &t, long long pid_begin,
+                               long long n, float *d_tab, size_t tab_floats, void *inst_host,
+                               float *tab_host);
+cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long nslots, void *d_ctr,
+                                long long total, int steps_per_launch, int block,
+                                cudaStream_t stream, long long *launches);
+
 class FastEngine {
 public:
     FastEngine() = default;

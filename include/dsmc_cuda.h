@@ -192,6 +192,37 @@ int dsmc_solve_host(dsmc_ctx *ctx, int path, const dsmc_params *p, const dsmc_su
                     const dsmc_collision *col, int64_t n, uint64_t *density_fx,
                     uint64_t *horizon_fx, dsmc_stats *stats);
 
+/* ---------------------------------------------------------------------------------------- */
+/* FAST_FP32 solve without any device allocation.                                            */
+/* (This entry point has no counterpart in the reference.)                                   */
+/*                                                                                           */
+/* For callers that cannot call cudaMalloc - code whose host framework owns all device       */
+/* memory through its own pool, or a plugin whose process intercepts or budgets allocation   */
+/* calls - but can pass device buffers they already hold. Solves the ballistic runner for    */
+/* particles [pid_begin, pid_begin + n) on the current device, like dsmc_run with            */
+/* DSMC_PATH_FAST_FP32, and returns when the solve is done.                                  */
+/*   surf     the surface with DEVICE pointers (T_map for the reference model; face_verts,   */
+/*            face_T, face_cdf (may be NULL), base_centroid, split_planes for the config     */
+/*            model), in the layouts of dsmc_surface.                                        */
+/*   density  device [hd*ftd*ffd] and horizon device [ftd*ffd] fixed-point grids: the solve  */
+/*            ADDS into them, so zero them first for a fresh result.                         */
+/*   stats    device [6] unsigned 64-bit counters in dsmc_stats order; zeroed by the call.   */
+/*   stream   a cudaStream_t, or NULL for the legacy default stream.                         */
+/* Scratch: one fixed device array of about 4.6 MB inside the library (at most 32,768       */
+/* resident particle slots and (hd+1) + (ftd+1) + 2 (ffd+1) + 1 <= 4096 table floats, ftd  */
+/* and ffd <= 255). Every GPU that loads the library holds that array until the process     */
+/* exits. Larger grids are rejected with DSMC_ERR_INVALID. The first call on a device looks  */
+/* up the array's device address (cudaGetSymbolAddress); make that first call before any     */
+/* stream capture. Every call shares the array and it keeps the last call's contents (the   */
+/* call resets what must start at zero): calls from this process are serialised, but calls  */
+/* whose GPU work overlaps - e.g. one issued while a previous one is still being replayed    */
+/* from a captured graph - race on the array. dsmc_noalloc_last_error() describes the last   */
+/* failure. */
+int dsmc_solve_fast_noalloc(const dsmc_params *p, const dsmc_surface *surf, int64_t pid_begin,
+                            int64_t n, uint64_t *density, uint64_t *horizon, uint64_t *stats,
+                            void *stream);
+const char *dsmc_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
