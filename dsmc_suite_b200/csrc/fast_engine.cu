@@ -21,10 +21,13 @@ namespace {
 
 constexpr float kPiF = 3.14159265358979f;
 
-__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
-    s = a + b;
-    const float bp = s - a;
-    e = (a - (s - bp)) + (b - bp);
+// Compensated accumulation hi + lo += b (Dekker's fast two-sum): exact when |hi| >= |b|, which
+// holds for position and velocity components except in the few steps where a component passes
+// through zero, whose error is then at most ulp(b) (< 1e-4 m or 1e-7 m/s here).
+__device__ __forceinline__ void accumulate(float &hi, float &lo, float b) {
+    const float t = hi + b;
+    lo += b - (t - hi);
+    hi = t;
 }
 
 // u in (0, 1): 24 random bits plus half an ulp, so 1 - u and u are never 0.
@@ -222,6 +225,70 @@ __device__ void enter_cell(const FastInst &I, Hot &h, Bounds &b, int cell) {
         h.nsig = static_cast<float>(__ldg(I.t.n_bg + h.ci) * I.p.cross_section);
 }
 
+// The particle left its cell: walk to the new cell one boundary at a time. Each move keeps the
+// shared boundary from the registers and loads only the next one, so a typical crossing costs
+// one table load. Same cells as track_shell / track_angles.
+__device__ __forceinline__ void move_cell(const FastInst &I, Hot &h, Bounds &b, float x, float y,
+                                          float r2, float zz) {
+    const int hd = I.p.hd, ftd = I.p.ftd, ffd = I.p.ffd;
+    int ht = h.cell >> 16, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
+    for (int it = 0; it < 64; it++) {
+        if (r2 > b.r2hi && ht + 1 < hd) {
+            ht++;
+            b.r2lo = b.r2hi;
+            b.r2hi = __ldg(I.rb2 + ht + 1);
+        } else if (r2 <= b.r2lo && ht > 0) {
+            ht--;
+            b.r2hi = b.r2lo;
+            b.r2lo = __ldg(I.rb2 + ht);
+        } else {
+            break;
+        }
+    }
+    for (int it = 0; it < 64; it++) {
+        if (zz > r2 * b.zhi && td + 1 < ftd) {
+            td++;
+            b.zlo = b.zhi;
+            b.zhi = __ldg(I.sbs + td + 1);
+        } else if (zz <= r2 * b.zlo && td > 0) {
+            td--;
+            b.zhi = b.zlo;
+            b.zlo = __ldg(I.sbs + td);
+        } else {
+            break;
+        }
+    }
+    for (int it = 0; it < 512; it++) {
+        if (x * b.c1 - y * b.s1 > 0.0f) {
+            fd = fd + 1 == ffd ? 0 : fd + 1;
+            b.s0 = b.s1;
+            b.c0 = b.c1;
+            const float2 q = __ldg(I.lonb + fd + 1);
+            b.s1 = q.x;
+            b.c1 = q.y;
+        } else if (x * b.c0 - y * b.s0 <= 0.0f && !(fd == 0 && x >= 0.0f && y > 0.0f)) {
+            fd = fd == 0 ? ffd - 1 : fd - 1;
+            b.s1 = b.s0;
+            b.c1 = b.c0;
+            const float2 q = __ldg(I.lonb + fd);
+            b.s0 = q.x;
+            b.c0 = q.y;
+        } else {
+            break;
+        }
+    }
+    const int cell = pack_cell(ht, td, fd);
+    if (cell == h.cell) return;
+    flush_cell(I, h);
+    h.cell = cell;
+    h.ci = (ht * ftd + td) * ffd + fd;
+    if (I.t.n_bg) {
+        h.nsig = 0.0f;
+        if (I.p.runner == DSMC_RUNNER_ADVANCED && ht < I.p.collide_ht_max && h.ci < I.t.n_bg_len)
+            h.nsig = static_cast<float>(__ldg(I.t.n_bg + h.ci) * I.p.cross_section);
+    }
+}
+
 __device__ __forceinline__ double cdf_eval(const double *coef, const double *box, int degree,
                                            double x) {
     const double t = (x - box[2]) / box[3];
@@ -374,27 +441,42 @@ __device__ bool launch(const FastArgs &a, long long i, const FastInst &I, Hot &h
         const float rot[3] = {omega * static_cast<float>(s[1]), -omega * static_cast<float>(s[0]), 0.0f};
 #pragma unroll
         for (int k = 0; k < 3; k++) v[k] = vn * n[k] + (sigma * t1) * e[k] + (sigma * t2) * nt[k] + rot[k];
-        // FP64 escape/bound classification of the launch
+        // FP64 escape/bound classification of the launch: E = v^2/2 - GM/r < 0 exactly when
+        // (v^2)^2 r^2 < (2 GM)^2, which needs no square root or division
         const double v2 = static_cast<double>(v[0]) * v[0] + static_cast<double>(v[1]) * v[1] +
                           static_cast<double>(v[2]) * v[2];
-        const double E = 0.5 * v2 - p.GM / sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
-        if (E < 0.0) st.bound++;
+        const double rr = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+        if (v2 * v2 * rr < 4.0 * p.GM * p.GM) st.bound++;
     }
     const double vd[3] = {v[0], v[1], v[2]};
     set_vel(h, vd);
-    const double R0 = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
-    const double g = p.GM / (R0 * R0 * R0);
-#pragma unroll
-    for (int k = 0; k < 3; k++) h.oa[k] = static_cast<float>(g * s[k]);
+    // old acceleration GM s / r^3 of the launch point (ballistic.c:176-181)
+    const float sx = h.sh[0] + h.sl[0], sy = h.sh[1] + h.sl[1], sz = h.sh[2] + h.sl[2];
+    const float ir = rsqrtf(fmaf(sx, sx, fmaf(sy, sy, sz * sz)));
+    const float g = static_cast<float>(p.GM) * (ir * ir * ir);
+    h.oa[0] = g * sx;
+    h.oa[1] = g * sy;
+    h.oa[2] = g * sz;
     h.hop = 0;
     return true;
+}
+
+// Cell of a launch point from the latitude and longitude the particle had when it landed,
+// starting in the lowest shell, moved by the comparison walks (no asin, atan2 or log).
+__device__ void enter_cell_near(const FastInst &I, Hot &h, Bounds &b) {
+    const float x = h.sh[0] + h.sl[0], y = h.sh[1] + h.sl[1], z = h.sh[2] + h.sl[2];
+    const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+    int ht = 0, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
+    track_shell(I, r2, ht);
+    track_angles(I, x, y, z, r2, td, fd);
+    enter_cell(I, h, b, pack_cell(ht, td, fd));
 }
 
 // Start of a hop (ballistic.c:124-181, advanced.c:271-333): weight and life checks, the
 // reference freeze scan, the launch and the starting cell. Returns 0 when the particle flies,
 // else its fate.
 __device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h, Bounds &b,
-                       StatAcc &st, float thi, float fi, float local_T) {
+                       StatAcc &st, float thi, float fi, float local_T, bool first) {
     const dsmc_params &p = I.p;
     const float W = weight(I, h);
     if (W < static_cast<float>(p.w_min)) return DSMC_FATE_PHOTOLYSED;
@@ -448,18 +530,30 @@ __device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h
         }
     }
     if (!launch(a, i, I, h, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
-    enter_cell(I, h, b, cell_from_scratch(I, h.sh[0] + h.sl[0], h.sh[1] + h.sl[1], h.sh[2] + h.sl[2]));
+    if (first)
+        enter_cell(I, h, b, cell_from_scratch(I, h.sh[0] + h.sl[0], h.sh[1] + h.sl[1], h.sh[2] + h.sl[2]));
+    else
+        enter_cell_near(I, h, b);
     return 0;
+}
+
+// Latitude and longitude of the current position in FP32 (the reference model's relaunch
+// angles, ballistic.c:245-247).
+__device__ __forceinline__ void angles_of_f(const Hot &h, float &thi, float &fi) {
+    const float x = h.sh[0] + h.sl[0], y = h.sh[1] + h.sl[1], z = h.sh[2] + h.sl[2];
+    thi = asinf(fminf(1.0f, fmaxf(-1.0f, z * rsqrtf(fmaf(x, x, fmaf(y, y, z * z))))));
+    fi = atan2f(x, y);
+    if (fi < 0.0f) fi += 2.0f * kPiF;
 }
 
 // Landing (ballistic.c:239-264): polar deposit (reference) or night freeze-out / day-side
 // re-emission point (config). Returns 0 to start a new hop, else the fate.
 __device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &local_T) {
     const dsmc_params &p = I.p;
-    angles_of(h, thi, fi);
     int td, fd;
-    ref_index(thi, fi, p.ftd, p.ffd, td, fd);
     if (p.model == DSMC_MODEL_REFERENCE) {
+        angles_of_f(h, thi, fi);
+        ref_index(thi, fi, p.ftd, p.ffd, td, fd);
         if (td <= 1 || td >= p.ftd - 2) {
             horizon_add(I, td, fd, 0.05f * weight(I, h));
             h.w0 *= 0.95f;
@@ -471,6 +565,8 @@ __device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &loc
     const double R = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
     double n[3] = {s[0] / R, s[1] / R, s[2] / R};
     if (n[0] * p.sun[0] + n[1] * p.sun[1] + n[2] * p.sun[2] <= 0.0) {
+        angles_of(h, thi, fi);
+        ref_index(thi, fi, p.ftd, p.ffd, td, fd);
         horizon_add(I, td, fd, weight(I, h));
         return DSMC_FATE_FROZEN;
     }
@@ -654,7 +750,7 @@ __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, St
                 I.t.ttime[6 * I.t.out_cap + slot] = local_T;
             }
         }
-        const int fate = hop_top(a, i, I, h, b, st, thi, fi, local_T);
+        const int fate = hop_top(a, i, I, h, b, st, thi, fi, local_T, true);
         if (fate == 0) return true;
         finish(a, i, I, h, st, fate);
     }
@@ -670,13 +766,8 @@ __device__ __forceinline__ void verlet_f32(Hot &h, float &x, float &y, float &z,
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         d[k] = fmaf(h.vh[k], dt, fmaf(h.vl[k], dt, -fmaf(acc[k], c1, h.oa[k] * c2)));
-        float t, e;
-        two_sum(h.sh[k], d[k], t, e);
-        h.sh[k] = t;
-        h.sl[k] += e;
-        two_sum(h.vh[k], -acc[k] * dt, t, e);
-        h.vh[k] = t;
-        h.vl[k] += e;
+        accumulate(h.sh[k], h.sl[k], d[k]);
+        accumulate(h.vh[k], h.vl[k], -acc[k] * dt);
         h.oa[k] = acc[k];
     }
     x = h.sh[0] + h.sl[0];
@@ -770,11 +861,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a)
             } else if (r2 >= re2) {
                 event = 2;
             } else {
-                int ht = h.cell >> 16, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
-                track_shell(*I, r2, ht);
-                track_angles(*I, x, y, z, r2, td, fd);
-                const int cell = pack_cell(ht, td, fd);
-                if (cell != h.cell) enter_cell(*I, h, b, cell);
+                move_cell(*I, h, b, x, y, r2, zz);
             }
         }
         if (!event) {
@@ -823,7 +910,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a)
             } else {
                 float thi, fi, local_T = 0.f;
                 fate = land(*I, h, thi, fi, local_T);
-                if (fate == 0) fate = hop_top(a, i, *I, h, b, st, thi, fi, local_T);
+                if (fate == 0) fate = hop_top(a, i, *I, h, b, st, thi, fi, local_T, false);
             }
             if (fate) {
                 finish(a, i, *I, h, st, fate);

@@ -92,9 +92,9 @@ public:
     long long slot_count() const { return nslots_; }
 
     // Launch shape (autotuned or set by the caller).
-    int block = 256;          // threads per block
+    int block = 128;          // threads per block
     int blocks_per_sm = 0;    // resident blocks per SM (0 = as many as fit)
-    int steps_per_launch = 2048;
+    int steps_per_launch = 4096;
     int launches_per_graph = 8;
     long long launches = 0;   // launches issued by the last run
 
