@@ -53,7 +53,9 @@ struct Hot {
     int nday, steps, hop;
     int cell;                  // packed (ht << 16) | (td << 8) | fd
     int ci;                    // (ht * ftd + td) * ffd + fd, -1 = none
-    unsigned long long acc;    // fixed-point deposits of cell ci not yet flushed
+    float run_w;               // weight-steps deposited in cell ci, not yet flushed
+    float W;                   // current weight: exact W0 2^(-c n_day) at cell changes and
+                               // events, times 2^(-c) per day-side step in between
     int hist_key, hist_cnt;
     int inst;                  // -1 = empty slot
 };
@@ -80,7 +82,8 @@ __device__ __forceinline__ void load_hot(const Slots &s, long long i, long long 
     h.hop = s.hop[i];
     h.cell = s.cell[i];
     h.ci = s.run_cell[i];
-    h.acc = s.run_acc[i];
+    h.run_w = s.run_w[i];
+    h.W = s.wcur[i];
     h.hist_key = s.hist_key[i];
     h.hist_cnt = s.hist_cnt[i];
     h.pcol = s.pcol[i];
@@ -104,7 +107,8 @@ __device__ __forceinline__ void store_hot(const Slots &s, long long i, long long
     s.hop[i] = h.hop;
     s.cell[i] = h.cell;
     s.run_cell[i] = h.ci;
-    s.run_acc[i] = h.acc;
+    s.run_w[i] = h.run_w;
+    s.wcur[i] = h.W;
     s.hist_key[i] = h.hist_key;
     s.hist_cnt[i] = h.hist_cnt;
     s.pcol[i] = h.pcol;
@@ -191,9 +195,13 @@ __device__ int cell_from_scratch(const FastInst &I, const float x, const float y
     return pack_cell(ht, td, fd);
 }
 
+// Flushes the weight-steps of the current cell as one 64-bit fixed-point atomic (W x 2^24
+// summed over the steps spent in the cell, rounded once). The float sum of a run is a function of
+// the particle's own trajectory only, so the grid stays independent of thread order.
 __device__ __forceinline__ void flush_cell(const FastInst &I, Hot &h) {
-    if (h.ci >= 0 && h.acc) atomicAdd(&I.t.density[h.ci], h.acc);
-    h.acc = 0;
+    if (h.ci >= 0 && h.run_w > 0.0f)
+        atomicAdd(&I.t.density[h.ci], __float2ull_rn(h.run_w * 16777216.0f));
+    h.run_w = 0.0f;
 }
 
 __device__ __forceinline__ void flush_hist(const FastInst &I, Hot &h) {
@@ -282,6 +290,7 @@ __device__ __forceinline__ void move_cell(const FastInst &I, Hot &h, Bounds &b, 
     flush_cell(I, h);
     h.cell = cell;
     h.ci = (ht * ftd + td) * ffd + fd;
+    h.W = h.w0 * exp2f(-I.c_day * static_cast<float>(h.nday));   // re-anchor the running weight
     if (I.t.n_bg) {
         h.nsig = 0.0f;
         if (I.p.runner == DSMC_RUNNER_ADVANCED && ht < I.p.collide_ht_max && h.ci < I.t.n_bg_len)
@@ -530,6 +539,10 @@ __device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h
         }
     }
     if (!launch(a, i, I, h, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
+    // the running weight restarts from its exact value at every launch (and at every cell
+    // change): points of the particle's own trajectory, so results do not depend on where
+    // kernel launches begin or end
+    h.W = weight(I, h);
     if (first)
         enter_cell(I, h, b, cell_from_scratch(I, h.sh[0] + h.sl[0], h.sh[1] + h.sl[1], h.sh[2] + h.sl[2]));
     else
@@ -701,7 +714,7 @@ __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, St
         h.hop = 0;
         h.pcol = 0.0f;
         h.ci = -1;
-        h.acc = 0;
+        h.run_w = 0.0f;
         h.hist_key = -1;
         h.hist_cnt = 0;
         const double zero[3] = {0.0, 0.0, 0.0};
@@ -778,10 +791,13 @@ __device__ __forceinline__ void verlet_f32(Hot &h, float &x, float &y, float &z,
 
 enum Flag { kRef = 1, kSkipFirst = 2, kCollide = 4, kHist = 8 };
 
-// kMinBlocks: resident 256-thread blocks per SM the register allocation must allow (2: up to
-// 128 registers a thread; 3: up to 80). The launch shape's blocks_per_sm picks the variant.
-template <int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a) {
+// kMaxThreads x kMinBlocks: the register budget the allocation must respect (65536 registers
+// per SM shared by kMinBlocks blocks of kMaxThreads). The launch shape picks the variant.
+// kLean: every instance of the launch is a config-model ballistic problem without speed
+// histograms whose hop cap is not below its life cap, so the reference-model, collision and
+// histogram branches and the per-hop step counter drop out of the loop.
+template <int kMaxThreads, int kMinBlocks, bool kLean>
+__global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const FastArgs a) {
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     Hot h;
     load_hot(a.s, i, a.nslots, h);
@@ -792,17 +808,17 @@ __global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a)
     if (alive) {
         // reload the cached bounds of the saved cell without flushing its pending deposits
         const int ci = h.ci;
-        const unsigned long long acc = h.acc;
+        const float run_w = h.run_w;
         h.ci = -1;
         enter_cell(a.inst[h.inst], h, b, h.cell);
         h.ci = ci;
-        h.acc = acc;
+        h.run_w = run_w;
     } else {
         alive = start_next(a, i, h, b, st);
     }
     int cur = -1, flags = 0, half_ffd = 0, life_cap = 0, hop_cap = 0, col_ht = 0, nbins = 0;
     float GM = 0.f, dt = 0.f, c1 = 0.f, c2 = 0.f, rl2 = 0.f, re2 = 0.f, cday = 0.f, sx = 0.f,
-          sy = 0.f, sz = 0.f, inv_bw = 0.f;
+          sy = 0.f, sz = 0.f, inv_bw = 0.f, fday = 0.f;
     const FastInst *I = nullptr;
     float x = 0.f, y = 0.f, z = 0.f, r2 = 0.f;
     bool fresh = true;
@@ -818,6 +834,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a)
             c1 = static_cast<float>(1.5 * p.dt_step * p.dt_step);
             c2 = static_cast<float>(p.dt_step * p.dt_step / 6.0);
             rl2 = I->r_land2;
+            fday = static_cast<float>(p.wdecay);
             re2 = I->r_esc2;
             cday = I->c_day;
             sx = static_cast<float>(p.sun[0]);
@@ -846,9 +863,9 @@ __global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a)
         float d[3];
         verlet_f32(h, x, y, z, r2, GM, dt, c1, c2, d);
         budget--;
-        const int ii = h.hop;
+        const int ii = kLean ? 1 : h.hop;
         h.steps++;
-        h.hop++;
+        if (!kLean) h.hop++;
         st.steps++;
         int event = 0;   // 1 landed (or hop cap), 2 escaped, 3 life cap
         const float zz = z * fabsf(z);
@@ -865,12 +882,15 @@ __global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a)
             }
         }
         if (!event) {
-            const bool day = (flags & kRef) ? ((h.cell & 0xff) < half_ffd)
-                                            : (fmaf(x, sx, fmaf(y, sy, z * sz)) > 0.0f);
-            h.nday += day;
-            if (!((flags & kSkipFirst) && ii == 0)) {
+            const bool day = (!kLean && (flags & kRef)) ? ((h.cell & 0xff) < half_ffd)
+                                                        : (fmaf(x, sx, fmaf(y, sy, z * sz)) > 0.0f);
+            if (day) {
+                h.nday++;
+                h.W *= fday;
+            }
+            if (kLean || !((flags & kSkipFirst) && ii == 0)) {
                 bool collided = false;
-                if ((flags & kCollide) && h.nsig > 0.0f) {
+                if (!kLean && (flags & kCollide) && h.nsig > 0.0f) {
                     h.pcol = fmaf(sqrtf(fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2]))), h.nsig, h.pcol);
                     if (h.pcol > h.pthr) {
                         const int ht = h.cell >> 16, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
@@ -882,9 +902,8 @@ __global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a)
                     }
                 }
                 if (!collided) {
-                    const float W = h.w0 * exp2f(-cday * static_cast<float>(h.nday));
-                    h.acc += __float2uint_rn(W * 16777216.0f);
-                    if (flags & kHist) {
+                    h.run_w += h.W;
+                    if (!kLean && (flags & kHist)) {
                         const float sp = sqrtf(fmaf(h.vh[0], h.vh[0], fmaf(h.vh[1], h.vh[1], h.vh[2] * h.vh[2])));
                         const int key = h.ci * nbins + min(static_cast<int>(sp * inv_bw), nbins - 1);
                         if (key == h.hist_key) {
@@ -898,7 +917,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) fast_kernel(const FastArgs a)
                 }
             }
             if (h.steps >= life_cap) event = 3;
-            else if (h.hop >= hop_cap) event = 1;
+            else if (!kLean && h.hop >= hop_cap) event = 1;
         }
         if (event) {
             fresh = true;
@@ -994,17 +1013,49 @@ void FastEngine::free_all() {
 namespace {
 
 // The two register budgets of fast_kernel (see kMinBlocks).
-void (*kernel_variant(int variant))(FastArgs) {
-    return variant >= 3 ? fast_kernel<3> : fast_kernel<2>;
+// Register budgets of fast_kernel: 0: 256 x 2 (128 registers a thread), 1: 256 x 3 (80),
+// 2: 128 x 3 (168), 3: 128 x 2 (255), 4: 128 x 4 (128).
+// The lean loop exists for budgets 0, 2 and 4.
+void (*kernel_variant(int variant, bool lean))(FastArgs) {
+    switch (variant) {
+        case 1: return fast_kernel<256, 3, false>;
+        case 2: return lean ? fast_kernel<128, 3, true> : fast_kernel<128, 3, false>;
+        case 3: return fast_kernel<128, 2, false>;
+        case 4: return lean ? fast_kernel<128, 4, true> : fast_kernel<128, 4, false>;
+        default: return lean ? fast_kernel<256, 2, true> : fast_kernel<256, 2, false>;
+    }
+}
+
+// Variant for a launch shape: blocks_per_sm names the register budget. The default (0) is the
+// fastest measured on B200: the lean loop fits 128 registers without spills (16 warps per SM),
+// the general loop needs 168 (12 warps per SM) to avoid them.
+int pick_variant(int block, int blocks_per_sm, bool lean) {
+    if (block > 128) return blocks_per_sm >= 3 ? 1 : 0;
+    if (blocks_per_sm == 2) return 3;
+    if (blocks_per_sm == 3) return 2;
+    if (blocks_per_sm == 4) return 4;
+    return lean ? 4 : 2;
+}
+
+// Whether every instance qualifies for the lean loop (see fast_kernel).
+bool all_lean(const std::vector<dsmc_params> &ps, const std::vector<DevTables> &ts) {
+    for (size_t k = 0; k < ps.size(); k++) {
+        const dsmc_params &p = ps[k];
+        if (p.model != DSMC_MODEL_CONFIG || p.runner != DSMC_RUNNER_BALLISTIC ||
+            p.skip_first_deposit || (ts[k].speed_hist && p.n_speed_bins > 0) ||
+            p.life_step_cap <= 0 || p.hop_step_cap < p.life_step_cap)
+            return false;
+    }
+    return true;
 }
 
 }  // namespace
 
 cudaError_t FastEngine::ensure_slots(int num_sms) {
     // one wave: as many blocks per SM as can be resident together
-    variant_ = blocks_per_sm >= 3 ? 3 : 2;
+    variant_ = pick_variant(block, blocks_per_sm, lean_);
     int resident = 0;
-    cudaError_t e0 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel_variant(variant_), block, 0);
+    cudaError_t e0 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel_variant(variant_, lean_), block, 0);
     if (e0 != cudaSuccess) return e0;
     if (resident < 1) return cudaErrorInvalidConfiguration;
     const int per_sm = (blocks_per_sm > resident || blocks_per_sm < 1) ? resident : blocks_per_sm;
@@ -1015,13 +1066,13 @@ cudaError_t FastEngine::ensure_slots(int num_sms) {
     if (slot_mem_) { cudaFree(slot_mem_); slot_mem_ = nullptr; }
     const long long S = want;
     // 4-byte fields: inst pid evt (3) + 15 vector floats + w0 nday steps hop cell run_cell
-    // hist_key hist_cnt pcol pthr ncol rest thi0 (13) = 31 words; plus run_acc (8 bytes).
+    // hist_key hist_cnt pcol pthr ncol rest wcur (13) = 31 words; plus run_w (8-byte slot).
     const size_t bytes = static_cast<size_t>(S) * (31 * 4 + 8) + 256;
     cudaError_t e = cudaMalloc(&slot_mem_, bytes);
     if (e != cudaSuccess) return e;
     char *b = static_cast<char *>(slot_mem_);
     auto take = [&](size_t each) { char *p = b; b += static_cast<size_t>(S) * each; return p; };
-    slots_.run_acc = reinterpret_cast<unsigned long long *>(take(8));
+    slots_.run_w = reinterpret_cast<float *>(take(8));
     slots_.inst = reinterpret_cast<int *>(take(4));
     slots_.pid = reinterpret_cast<unsigned *>(take(4));
     slots_.evt = reinterpret_cast<unsigned *>(take(4));
@@ -1042,7 +1093,7 @@ cudaError_t FastEngine::ensure_slots(int num_sms) {
     slots_.pthr = reinterpret_cast<float *>(take(4));
     slots_.ncol = reinterpret_cast<int *>(take(4));
     slots_.rest = reinterpret_cast<float *>(take(4));
-    slots_.thi0 = reinterpret_cast<float *>(take(4));
+    slots_.wcur = reinterpret_cast<float *>(take(4));
     nslots_ = S;
     if (!d_ctr_) {
         if ((e = cudaMalloc(&d_ctr_, sizeof(FastCounters))) != cudaSuccess) return e;
@@ -1157,13 +1208,14 @@ cudaError_t FastEngine::drain(long long total, cudaStream_t stream) {
     a.K = steps_per_launch;
     const unsigned grid = static_cast<unsigned>(nslots_ / block);
     const int key[4] = {static_cast<int>(total & 0x7fffffff), static_cast<int>(total >> 31),
-                        ninst_ * 8 + variant_, steps_per_launch * 64 + launches_per_graph};
+                        (ninst_ * 8 + variant_) * 2 + (lean_ ? 1 : 0),
+                        steps_per_launch * 64 + launches_per_graph};
     const bool use_graph = launches_per_graph > 1;
     if (use_graph && (!graph_ || graph_stream_ != stream || std::memcmp(key, graph_key_, sizeof key) != 0)) {
         if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
         cudaGraph_t g;
         if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-        for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_)<<<grid, block, 0, stream>>>(a);
+        for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_, lean_)<<<grid, block, 0, stream>>>(a);
         if ((e = cudaStreamEndCapture(stream, &g)) != cudaSuccess) return e;
         e = cudaGraphInstantiate(&graph_, g, 0);
         cudaGraphDestroy(g);
@@ -1182,7 +1234,7 @@ cudaError_t FastEngine::drain(long long total, cudaStream_t stream) {
             if ((e = cudaGraphLaunch(graph_, stream)) != cudaSuccess) return e;
             launches += launches_per_graph;
         } else {
-            kernel_variant(variant_)<<<grid, block, 0, stream>>>(a);
+            kernel_variant(variant_, lean_)<<<grid, block, 0, stream>>>(a);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             launches += 1;
         }
@@ -1199,6 +1251,7 @@ cudaError_t FastEngine::run(const dsmc_params &p, const DevTables &t, bool fp64,
                             long long n, int num_sms, cudaStream_t stream) {
     if (fp64) return cudaErrorNotSupported;
     if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767) return cudaErrorInvalidValue;
+    lean_ = all_lean({p}, {t});
     cudaError_t e = ensure_slots(num_sms);
     if (e != cudaSuccess) return e;
     e = upload_instances({p}, {t}, {n}, {pid_begin}, stream);
@@ -1210,6 +1263,7 @@ cudaError_t FastEngine::run_batch(const std::vector<dsmc_params> &ps, const std:
                                   const std::vector<long long> &counts, int num_sms, cudaStream_t stream) {
     for (const auto &p : ps)
         if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767) return cudaErrorInvalidValue;
+    lean_ = all_lean(ps, ts);
     cudaError_t e = ensure_slots(num_sms);
     if (e != cudaSuccess) return e;
     std::vector<long long> pid0(ps.size(), 0);
@@ -1281,7 +1335,7 @@ cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long ns
     char *b = static_cast<char *>(slot_mem);
     auto take = [&](size_t each) { char *q = b; b += static_cast<size_t>(S) * each; return q; };
     Slots s{};
-    s.run_acc = reinterpret_cast<unsigned long long *>(take(8));
+    s.run_w = reinterpret_cast<float *>(take(8));
     s.inst = reinterpret_cast<int *>(take(4));
     s.pid = reinterpret_cast<unsigned *>(take(4));
     s.evt = reinterpret_cast<unsigned *>(take(4));
@@ -1302,7 +1356,7 @@ cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long ns
     s.pthr = reinterpret_cast<float *>(take(4));
     s.ncol = reinterpret_cast<int *>(take(4));
     s.rest = reinterpret_cast<float *>(take(4));
-    s.thi0 = reinterpret_cast<float *>(take(4));
+    s.wcur = reinterpret_cast<float *>(take(4));
     cudaError_t e;
     if ((e = cudaMemsetAsync(d_ctr, 0, sizeof(FastCounters), stream)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(s.inst, 0xff, S * sizeof(int), stream)) != cudaSuccess) return e;
@@ -1320,7 +1374,7 @@ cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long ns
     long long stalled = 0;
     for (;;) {
         if (stalled > 4096) return cudaErrorLaunchTimeout;
-        fast_kernel<2><<<grid, block, 0, stream>>>(a);
+        fast_kernel<256, 2, false><<<grid, block, 0, stream>>>(a);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         *launches += 1;
         if ((e = cudaMemcpyAsync(&host, d_ctr, sizeof host, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)

@@ -38,13 +38,13 @@ struct Slots {
     int *hop;                // steps in the current hop
     int *cell;               // packed (ht << 16) | (td << 8) | fd
     int *run_cell;           // cell of the register deposit run, -1 = none
-    unsigned long long *run_acc;
+    float *run_w;            // weight-steps in run_cell not yet flushed (8-byte slot reserved)
     int *hist_key;           // (cell * nbins + bin) of the speed-histogram run, -1 = none
     int *hist_cnt;
     float *pcol, *pthr;      // accumulated collision probability and its threshold
     int *ncol;
     float *rest;             // freeze waiting time (reference model)
-    float *thi0;             // launch latitude of the particle (for ttime row 0)
+    float *wcur;             // running weight (the hot loop's W between launches)
 };
 
 struct FastCounters {
@@ -94,7 +94,7 @@ public:
     // Launch shape (autotuned or set by the caller).
     int block = 128;          // threads per block
     int blocks_per_sm = 0;    // resident blocks per SM (0 = as many as fit)
-    int steps_per_launch = 4096;
+    int steps_per_launch = 8192;
     int launches_per_graph = 8;
     long long launches = 0;   // launches issued by the last run
 
@@ -122,6 +122,7 @@ private:
     int graph_key_[4] = {0, 0, 0, 0};
     bool nslots_want_changed_ = false;
     int variant_ = 2;
+    bool lean_ = false;
 };
 
 }  // namespace dsmc
