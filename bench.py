@@ -51,6 +51,14 @@ def args_parse():
                     help="launch shape block,blocks_per_sm,steps_per_launch,launches_per_graph")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mode", choices=["solve", "batch", "serve"], default="solve",
+                    help="solve: one config-1 solve per step (default); batch: the 64-instance "
+                         "batch; serve: the Poisson request stream")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
+    ap.add_argument("--seconds", type=float, default=60.0, help="serve: arrival window [s]")
+    ap.add_argument("--sample", type=float, default=0.05,
+                    help="serve: fraction of requests re-solved with the plain FP64 path")
+    ap.add_argument("--budget-gb", type=float, default=80.0, help="batch/serve: HBM budget")
     return ap.parse_args()
 
 
@@ -201,10 +209,213 @@ def run_reference_arm(a):
     print(json.dumps(line), flush=True)
 
 
+def fma_peak(N, device: int, fp64: bool) -> float:
+    import ctypes
+    from dsmc_suite_b200 import Context
+    with Context(device) as c:
+        v = ctypes.c_double()
+        N.check(N.lib().dsmc_measure_fma_peak(c.h, int(fp64), ctypes.byref(v)), "fma peak", c.h)
+        return v.value
+
+
+def plain_fp64_rate(N, device: int, problems, limit_steps: float = 4e11):
+    """Plain FP64 path (one thread per particle, the reference's arithmetic) over the same
+    problems, one solve after another, timed with CUDA events on a dedicated stream; stops
+    after about limit_steps particle-steps. Returns (steps/s, problems solved)."""
+    import torch
+    from dsmc_suite_b200 import Context
+    stream = torch.cuda.Stream()
+    steps, ms, k = 0, 0.0, 0
+    with torch.cuda.stream(stream), Context(device) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        for P in problems:
+            ctx.setup(P.params, P.surface, P.collision)
+            ctx.zero()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.run(N.PATH_PLAIN_FP64, 0, P.n)
+            e1.record(stream)
+            stream.synchronize()
+            ms += e0.elapsed_time(e1)
+            steps += ctx.stats()["total_steps"]
+            k += 1
+            if steps >= limit_steps:
+                break
+    return steps / (ms * 1e-3), k
+
+
+BATCH_CONFIG = {"workload": "config-3 batch: 64 ballistic exospheres in one queue; particles "
+                            "lognormal median 3e5 sigma_ln 1.17 clipped [1e4, 1e7]; bodies "
+                            "Ceres/Europa/Moon; sub-solar T U(100,400) K, longitude uniform; "
+                            "20-60 exp shells x 36 x 72; dt 2 s, <=20000 steps",
+                "solver": "dsmc_server: FAST_FP32 resident slots, one device work queue, "
+                          "rounds replayed as a CUDA graph",
+                "l2": "fresh grids every step; 256 MiB L2 flush before each step", "seed": SEED}
+
+
+def run_batch_mode(a):
+    """Config 3: every step submits the 64 instances and polls until all are fetched.
+    value = particle-steps / device time of the rounds (CUDA events); e2e = the same steps /
+    wall time of submit (host tables -> device) ... fetch (grids -> host)."""
+    import torch
+    from dsmc_suite_b200 import _native as N, Server
+    from dsmc_suite_b200 import workloads as W
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    probs = W.batch_instances(SEED, 64)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    srv = Server(local, hbm_budget=int(a.budget_gb * 1e9), max_requests=4096)
+    if a.shape:
+        shape = [int(v) for v in a.shape.split(",")]
+        srv.set_shape(*shape)
+        BATCH_CONFIG["launch_shape"] = shape
+
+    def step():
+        i0 = srv.info()
+        t0 = time.perf_counter()
+        for P in probs:
+            srv.submit(P.params, P.surface, P.n, P.collision)
+        res = srv.run_all()
+        wall = time.perf_counter() - t0
+        i1 = srv.info()
+        steps = sum(r["stats"]["total_steps"] for r in res.values())
+        h2d = sum(P.surface.face_T.nbytes + P.surface.ico.face_verts.nbytes +
+                  P.surface.ico.split_planes.nbytes + P.surface.ico.base_centroid.nbytes
+                  for P in probs)
+        d2h = sum(r["density"].nbytes + r["horizon"].nbytes for r in res.values())
+        return steps, i1["busy_ms"] - i0["busy_ms"], wall, i1["launches"] - i0["launches"], h2d, d2h
+
+    for _ in range(a.warmup):
+        step()
+    tot = [0, 0.0, 0.0, 0, 0, 0]
+    with ClockSampler(local) as clocks:
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = step()
+            tot = [x + y for x, y in zip(tot, r)]
+    steps, busy_ms, wall, launches, h2d, d2h = tot
+    value = steps / (busy_ms * 1e-3)
+    info = srv.info()
+    srv.close()
+    plain, nplain = plain_fp64_rate(N, local, probs)
+    peak = fma_peak(N, local, False)
+    achieved = value * FLOPS_PER_STEP / 1e12
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": busy_ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": dict(BATCH_CONFIG, instances=len(probs),
+                           particles=int(sum(P.n for P in probs))),
+            "particle_steps_per_step": steps / a.steps, "gpu_launches": launches,
+            "resident_slots": info["slots"], "clocks": clocks.summary(),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured in this run: FP32 FMA-chain kernel",
+                         "algorithmic_flops_per_step": FLOPS_PER_STEP},
+            "e2e": {"value": steps / wall, "unit": METRIC, "h2d_bytes_per_step": h2d // a.steps,
+                    "d2h_bytes_per_step": d2h // a.steps,
+                    "api": "dsmc_server_submit/poll/fetch (C ABI, host buffers)",
+                    "seconds": wall},
+            "plain_fp64": {"value": plain, "unit": METRIC, "instances": nplain,
+                           "note": "same instances, solved one after another"},
+            "speedup_vs_plain_fp64": value / plain}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve_mode(a):
+    """Config 4: Poisson arrivals; each request is admitted at the first poll after its arrival
+    (or later, when the budget refuses it), and its latency runs from arrival to the poll that
+    saw it complete. Throughput = particle-steps of the completed requests / wall time from the
+    first arrival to the last completion."""
+    import torch
+    from dsmc_suite_b200 import _native as N, Context, Server, BudgetExceeded
+    from dsmc_suite_b200 import workloads as W
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(local)
+    with Context(local) as ctx:
+        t_prep = time.perf_counter()
+        stream = W.served_stream(ctx, a.rate, a.seconds, SEED)
+        t_prep = time.perf_counter() - t_prep
+    rng = np.random.default_rng(SEED + 1)
+    sample = set(int(i) for i in np.nonzero(rng.uniform(size=len(stream)) < a.sample)[0])
+    srv = Server(local, hbm_budget=int(a.budget_gb * 1e9), max_requests=len(stream) + 16)
+    if a.shape:
+        srv.set_shape(*[int(v) for v in a.shape.split(",")])
+    i0 = srv.info()
+    backlog: list[int] = []      # indices refused by admission, retried in order
+    ticket_of: dict[int, int] = {}
+    done: dict[int, dict] = {}
+    nxt = 0
+    refused = 0
+    t0 = srv.now()
+    with ClockSampler(local) as clocks:
+        while len(done) < len(stream):
+            now = srv.now()
+            while nxt < len(stream) and t0 + stream[nxt][0] <= now:
+                backlog.append(nxt)
+                nxt += 1
+            while backlog:
+                k = backlog[0]
+                P = stream[k][1]
+                try:
+                    ticket_of[srv.submit(P.params, P.surface, P.n, P.collision)] = k
+                except BudgetExceeded:
+                    refused += 1
+                    break
+                backlog.pop(0)
+            for t in srv.poll():
+                k = ticket_of[t]
+                r = srv.fetch(t, grids=k in sample)
+                r["arrival"] = t0 + stream[k][0]
+                done[k] = r
+            if srv.info()["active"] == 0 and not backlog and nxt < len(stream):
+                time.sleep(max(0.0, min(0.005, t0 + stream[nxt][0] - srv.now())))
+    t_end = max(r["t_done"] for r in done.values())
+    info = srv.info()
+    srv.close()
+    lat = np.array([r["t_done"] - r["arrival"] for r in done.values()])
+    steps = sum(r["stats"]["total_steps"] for r in done.values())
+    wall = t_end - t0
+    # density error of the served FP32 results against the plain FP64 path, seeded subsample
+    errs = []
+    with Context(local) as ctx:
+        for k in sorted(sample):
+            P = stream[k][1]
+            g = ctx.solve(N.PATH_PLAIN_FP64, P.params, P.surface, P.n, collision=P.collision)
+            errs.append(W.rel_l2(done[k]["density"], g["density"]))
+    kinds = [stream[k][1].meta["kind"] for k in range(len(stream))]
+    line = {"metric": METRIC, "value": steps / wall, "unit": METRIC, "n_gpus": 1, "steps": 1,
+            "warmup": 0, "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": f"config-4 served stream: Poisson {a.rate:g} req/s for "
+                                   f"{a.seconds:g} s, 70/30 ballistic/collisional, config-3 "
+                                   f"distributions, own seed per request",
+                       "budget_gb": a.budget_gb, "requests": len(stream),
+                       "collisional": kinds.count("collisional"), "seed": SEED},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "mean": float(lat.mean()), "max": float(lat.max())},
+            "device_busy_frac": (info["busy_ms"] - i0["busy_ms"]) * 1e-3 / wall,
+            "gpu_launches": info["launches"] - i0["launches"], "rounds": info["rounds"] - i0["rounds"],
+            "admission_refusals": refused, "particles": int(sum(r["n"] for r in done.values())),
+            "density_rel_l2_vs_fp64": {"sample": len(errs), "median": float(np.median(errs)) if errs else None,
+                                       "max": float(np.max(errs)) if errs else None},
+            "prep_seconds": t_prep, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = args_parse()
     if a.impl == "reference":
         return run_reference_arm(a)
+    if a.mode == "batch":
+        return run_batch_mode(a)
+    if a.mode == "serve":
+        return run_serve_mode(a)
     import torch
     import torch.distributed as dist
     from datetime import timedelta

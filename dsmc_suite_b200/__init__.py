@@ -15,8 +15,9 @@ from ._native import (DsmcError, Icosphere, SurfaceInputs, CollisionInputs, para
                       RUNNER_BALLISTIC, RUNNER_ADVANCED, PATH_PLAIN_FP64, PATH_FAST_FP32,
                       PATH_FAST_FP64, FIXED_SCALE)
 from .solver import Context
+from .server import BudgetExceeded, Server
 
-__all__ = ["Context", "DsmcError", "Icosphere", "SurfaceInputs", "CollisionInputs",
+__all__ = ["Context", "Server", "BudgetExceeded", "DsmcError", "Icosphere", "SurfaceInputs", "CollisionInputs",
            "params_config", "params_reference", "latlon_temperature", "run_ballistic",
            "run_advanced", "MODEL_REFERENCE", "MODEL_CONFIG", "RUNNER_BALLISTIC",
            "RUNNER_ADVANCED", "PATH_PLAIN_FP64", "PATH_FAST_FP32", "PATH_FAST_FP64",

@@ -85,6 +85,22 @@ class Stats(C.Structure):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
+class ServerInfo(C.Structure):
+    """dsmc_server_info."""
+    _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "fetched", "rejected", "active",
+                                          "bytes_in_use", "bytes_budget", "slots", "rounds",
+                                          "launches", "total_steps")] + [("busy_ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class RequestInfo(C.Structure):
+    """dsmc_request_info."""
+    _fields_ = [("n", C.c_int64), ("ncell", C.c_int64), ("nhcell", C.c_int64),
+                ("t_submit", C.c_double), ("t_done", C.c_double)]
+
+
 def ptr(a: np.ndarray | None, ctype=C.c_double):
     """Pointer to a contiguous numpy array (or NULL)."""
     if a is None:
@@ -143,6 +159,17 @@ SIGNATURES = [
     ("dsmc_solve_fast_noalloc", C.c_int, [C.POINTER(Params), C.POINTER(Surface), C.c_int64,
                                           C.c_int64, _U64P, _U64P, _U64P, _P]),
     ("dsmc_noalloc_last_error", C.c_char_p, []),
+    ("dsmc_server_create", C.c_int, [C.c_int, C.c_int64, C.c_int, C.POINTER(_P)]),
+    ("dsmc_server_destroy", C.c_int, [_P]),
+    ("dsmc_server_last_error", C.c_char_p, [_P]),
+    ("dsmc_server_set_shape", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("dsmc_server_submit", C.c_int, [_P, C.POINTER(Params), C.POINTER(Surface),
+                                     C.POINTER(Collision), C.c_int64, _I64P]),
+    ("dsmc_server_poll", C.c_int, [_P, _I64P, C.c_int, C.POINTER(C.c_int)]),
+    ("dsmc_server_fetch", C.c_int, [_P, C.c_int64, _U64P, _U64P, C.POINTER(Stats),
+                                    C.POINTER(RequestInfo)]),
+    ("dsmc_server_info_get", C.c_int, [_P, C.POINTER(ServerInfo)]),
+    ("dsmc_server_now", C.c_double, [_P]),
     ("dsmc_solve_host", C.c_int, [_P, C.c_int, C.POINTER(Params), C.POINTER(Surface),
                                   C.POINTER(Collision), C.c_int64, _U64P, _U64P, C.POINTER(Stats)]),
 ]

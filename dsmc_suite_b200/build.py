@@ -37,6 +37,8 @@ CUDA_SOURCES = {
     "fast_engine.cu": [],
     "kernel_peak.cu": [],
     "noalloc.cu": [],
+    "problem.cu": [],
+    "server.cu": [],
     "dsmc_abi.cu": [],
 }
 C_SOURCES = ["host_setup.c", "host_scalar.c", "host_fileio.c", "host_runners.c"]

@@ -10,6 +10,7 @@
 #include "dsmc_cuda.h"
 #include "dsmc_kernels.h"
 #include "fast_engine.h"
+#include "problem.h"
 
 extern "C" {
 #include "types.h"
@@ -27,7 +28,7 @@ struct dsmc_ctx {
     dsmc_params params{};
     DevTables t{};
     long long ncell = 0, nhcell = 0, nhist = 0;
-    std::vector<void *> tables;     // owned device allocations of the current problem
+    dsmc::Problem prob;             // tables and grids of the current problem
     void *outputs[3] = {nullptr, nullptr, nullptr};  // ttime, fate, steps
     unsigned long long *stats = nullptr;
     dsmc::FastEngine *fast = nullptr;
@@ -63,8 +64,7 @@ int set_device(dsmc_ctx *c) {
 }
 
 void free_tables(dsmc_ctx *c) {
-    for (void *p : c->tables) cudaFree(p);
-    c->tables.clear();
+    c->prob.release();
     c->ready = false;
 }
 
@@ -78,60 +78,6 @@ void free_outputs(dsmc_ctx *c) {
     c->t.steps = nullptr;
     c->t.out_cap = 0;
     c->t.out_base = 0;
-}
-
-// Allocate and upload one host array (nullptr host -> nullptr device).
-template <typename T, typename D>
-int upload(dsmc_ctx *c, const T *host, size_t count, D **dev) {
-    static_assert(sizeof(T) == sizeof(D), "element size mismatch");
-    *dev = nullptr;
-    if (!host || count == 0) return DSMC_OK;
-    void *p = nullptr;
-    DSMC_CUDA_TRY(c, cudaMalloc(&p, count * sizeof(T)));
-    c->tables.push_back(p);
-    DSMC_CUDA_TRY(c, cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
-    *dev = static_cast<D *>(p);
-    return DSMC_OK;
-}
-
-template <typename T>
-int alloc_zero(dsmc_ctx *c, size_t count, T **dev) {
-    void *p = nullptr;
-    DSMC_CUDA_TRY(c, cudaMalloc(&p, count * sizeof(T)));
-    c->tables.push_back(p);
-    DSMC_CUDA_TRY(c, cudaMemsetAsync(p, 0, count * sizeof(T), c->stream));
-    *dev = static_cast<T *>(p);
-    return DSMC_OK;
-}
-
-int check_params(dsmc_ctx *c, const dsmc_params *p, const dsmc_surface *s,
-                 const dsmc_collision *col) {
-    if (!p || !s) return fail(c, DSMC_ERR_INVALID, "params and surface are required");
-    if (p->ftd < 1 || p->ffd < 1 || p->hd < 1 || p->ftd > 4096 || p->ffd > 4096 || p->hd > 4096)
-        return fail(c, DSMC_ERR_INVALID, "grid dimensions out of range");
-    if (!(p->dt_step > 0.0) || !(p->Radii > 0.0) || !(p->GM > 0.0) || !(p->max_height > p->Radii))
-        return fail(c, DSMC_ERR_INVALID, "dt, Radii, GM and max_height must be positive");
-    if (p->hop_step_cap < 1) return fail(c, DSMC_ERR_INVALID, "hop_step_cap must be >= 1");
-    if (p->model == DSMC_MODEL_REFERENCE) {
-        if (!s->T_map) return fail(c, DSMC_ERR_INVALID, "reference model needs T_map");
-    } else if (p->model == DSMC_MODEL_CONFIG) {
-        if (!s->face_verts || !s->face_T || !s->base_centroid || !s->split_planes ||
-            s->nlevel < 0 || s->nlevel > 6 || s->nface != (20 << (2 * s->nlevel)))
-            return fail(c, DSMC_ERR_INVALID, "config model needs a complete icosphere surface");
-    } else {
-        return fail(c, DSMC_ERR_INVALID, "unknown model %d", p->model);
-    }
-    if (p->runner != DSMC_RUNNER_BALLISTIC && p->runner != DSMC_RUNNER_ADVANCED)
-        return fail(c, DSMC_ERR_INVALID, "unknown runner %d", p->runner);
-    if (col && col->n_bg) {
-        if (!col->cdf_coef || !col->cdf_box || !col->cdf_total || !col->cdf_valid ||
-            col->cdf_degree < 0 || col->cdf_degree > DSMC_CDF_MAX_DEGREE || col->n_bg_len < 0)
-            return fail(c, DSMC_ERR_INVALID, "incomplete collision tables");
-    }
-    if (p->n_speed_bins < 0 || p->n_speed_bins > 1024 ||
-        (p->n_speed_bins > 0 && !(p->speed_bin_width > 0.0)))
-        return fail(c, DSMC_ERR_INVALID, "bad speed histogram shape");
-    return DSMC_OK;
 }
 
 }  // namespace
@@ -209,73 +155,28 @@ int dsmc_ctx_set_stream(dsmc_ctx *c, void *stream) {
 int dsmc_setup(dsmc_ctx *c, const dsmc_params *p, const dsmc_surface *s,
                const dsmc_collision *col) {
     if (!c) return DSMC_ERR_INVALID;
-    int rc = check_params(c, p, s, col);
+    int rc = dsmc::problem_check(p, s, col, c->err, sizeof c->err);
     if (rc != DSMC_OK) return rc;
     if ((rc = set_device(c)) != DSMC_OK) return rc;
     DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     free_tables(c);
-    DevTables &t = c->t;
-    const double *out_ttime = t.ttime;
-    int *out_fate = t.fate;
-    long long *out_steps = t.steps;
-    long long out_cap = t.out_cap;
-    t = DevTables{};
-    t.ttime = const_cast<double *>(out_ttime);
-    t.fate = out_fate;
-    t.steps = out_steps;
-    t.out_cap = out_cap;
-    c->params = *p;
-    const long long ftd = p->ftd, ffd = p->ffd, hd = p->hd;
-    c->ncell = hd * ftd * ffd;
-    c->nhcell = ftd * ffd;
-    c->nhist = p->n_speed_bins > 0 ? c->ncell * p->n_speed_bins : 0;
-
-    if (p->model == DSMC_MODEL_REFERENCE) {
-        // Launch-speed table, built on the host with the reference's constants
-        // (include/constants.h:17-23 and src/common/velocity.c:6-47).
-        static VelocityTable vt;
-        velocity_table_init(&vt, 18e-3, 6.02e23, 1.38e-23);
-        const double *d_T = nullptr;
-        if ((rc = upload(c, s->T_map, static_cast<size_t>(ftd * ffd), &d_T)) != DSMC_OK) return rc;
-        t.T_map = d_T;
-        double *d_sp = nullptr;
-        int *d_cnt = nullptr;
-        if ((rc = upload(c, &vt.speeds[0][0], 23 * 1000, &d_sp)) != DSMC_OK) return rc;
-        if ((rc = upload(c, vt.count, 23, &d_cnt)) != DSMC_OK) return rc;
-        // The upload is asynchronous: keep the static table stable until the copy is done.
-        DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-        t.vt_speeds = d_sp;
-        t.vt_count = d_cnt;
-    } else {
-        const size_t nf = static_cast<size_t>(s->nface);
-        const size_t nnode = static_cast<size_t>(20 * ((1 << (2 * s->nlevel)) - 1) / 3);
-        t.nface = s->nface;
-        t.nlevel = s->nlevel;
-        const double *dv = nullptr, *dT = nullptr, *dc = nullptr, *db = nullptr, *dp = nullptr;
-        if ((rc = upload(c, s->face_verts, nf * 9, &dv)) != DSMC_OK) return rc;
-        if ((rc = upload(c, s->face_T, nf, &dT)) != DSMC_OK) return rc;
-        if ((rc = upload(c, s->face_cdf, nf, &dc)) != DSMC_OK) return rc;
-        if ((rc = upload(c, s->base_centroid, static_cast<size_t>(60), &db)) != DSMC_OK) return rc;
-        if ((rc = upload(c, s->split_planes, nnode * 9, &dp)) != DSMC_OK) return rc;
-        t.face_verts = dv; t.face_T = dT; t.face_cdf = dc; t.base_centroid = db; t.split_planes = dp;
-    }
-    if (col && col->n_bg) {
-        const size_t nc = static_cast<size_t>(c->ncell);
-        const double *nb = nullptr, *cc = nullptr, *cb = nullptr, *ct = nullptr;
-        const int *cv = nullptr;
-        if ((rc = upload(c, col->n_bg, static_cast<size_t>(col->n_bg_len), &nb)) != DSMC_OK) return rc;
-        if ((rc = upload(c, col->cdf_coef, nc * DSMC_CDF_STRIDE, &cc)) != DSMC_OK) return rc;
-        if ((rc = upload(c, col->cdf_box, nc * 4, &cb)) != DSMC_OK) return rc;
-        if ((rc = upload(c, col->cdf_total, nc, &ct)) != DSMC_OK) return rc;
-        if ((rc = upload(c, reinterpret_cast<const int *>(col->cdf_valid), nc, &cv)) != DSMC_OK) return rc;
-        t.n_bg = nb; t.n_bg_len = col->n_bg_len; t.cdf_coef = cc; t.cdf_box = cb; t.cdf_total = ct;
-        t.cdf_valid = cv; t.cdf_degree = col->cdf_degree;
-    }
-    if ((rc = alloc_zero(c, static_cast<size_t>(c->ncell), &t.density)) != DSMC_OK) return rc;
-    if ((rc = alloc_zero(c, static_cast<size_t>(c->nhcell), &t.horizon)) != DSMC_OK) return rc;
-    if (c->nhist > 0 && (rc = alloc_zero(c, static_cast<size_t>(c->nhist), &t.speed_hist)) != DSMC_OK)
+    rc = dsmc::problem_build(c->prob, p, s, col, c->stats, c->stream, false, c->err, sizeof c->err);
+    if (rc != DSMC_OK) {
+        free_tables(c);
         return rc;
-    t.stats = c->stats;
+    }
+    // keep the per-particle output buffers of dsmc_enable_particle_outputs
+    DevTables &t = c->t;
+    const DevTables old = t;
+    t = c->prob.t;
+    t.ttime = old.ttime;
+    t.fate = old.fate;
+    t.steps = old.steps;
+    t.out_cap = old.out_cap;
+    c->params = *p;
+    c->ncell = c->prob.ncell;
+    c->nhcell = c->prob.nhcell;
+    c->nhist = c->prob.nhist;
     DSMC_CUDA_TRY(c, cudaMemsetAsync(c->stats, 0, dsmc::kStatCount * sizeof(unsigned long long), c->stream));
     DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->ready = true;

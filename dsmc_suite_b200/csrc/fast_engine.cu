@@ -35,13 +35,12 @@ __device__ __forceinline__ float unit_open(uint32_t w) {
     return (static_cast<float>(w >> 8) + 0.5f) * (1.0f / 16777216.0f);
 }
 
+// Kernel arguments; the queue's size (total work items, instances) is read from the counters.
 struct FastArgs {
     const FastInst *inst;
-    int ninst;
     Slots s;
     long long nslots;
     FastCounters *ctr;
-    long long total;
     int K;
 };
 
@@ -680,7 +679,7 @@ __device__ __forceinline__ unsigned long long grab_work(FastCounters *ctr) {
 }
 
 __device__ __forceinline__ int find_inst(const FastArgs &a, unsigned long long w) {
-    int lo = 0, hi = a.ninst - 1;
+    int lo = 0, hi = static_cast<int>(a.ctr->ninst) - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (static_cast<unsigned long long>(a.inst[mid].work_base) <= w) lo = mid;
@@ -695,7 +694,7 @@ __device__ __forceinline__ int find_inst(const FastArgs &a, unsigned long long w
 __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, StatAcc &st) {
     for (;;) {
         const unsigned long long w = grab_work(a.ctr);
-        if (w >= static_cast<unsigned long long>(a.total)) return false;
+        if (w >= a.ctr->total) return false;
         const int ii = find_inst(a, w);
         const FastInst &I = a.inst[ii];
         const dsmc_params &p = I.p;
@@ -1007,12 +1006,18 @@ void FastEngine::free_all() {
     d_ctr_ = nullptr;
     if (h_ctr_) cudaFreeHost(h_ctr_);
     h_ctr_ = nullptr;
+    if (d_stats_) cudaFree(d_stats_);
+    d_stats_ = nullptr;
+    stats_cap_ = 0;
+    ninst_cap_ = 0;
+    for (void *p : inst_tabs_)
+        if (p) cudaFree(p);
+    inst_tabs_.clear();
     nslots_ = 0;
 }
 
 namespace {
 
-// The two register budgets of fast_kernel (see kMinBlocks).
 // Register budgets of fast_kernel: 0: 256 x 2 (128 registers a thread), 1: 256 x 3 (80),
 // 2: 128 x 3 (168), 3: 128 x 2 (255), 4: 128 x 4 (128).
 // The lean loop exists for budgets 0, 2 and 4.
@@ -1192,37 +1197,68 @@ cudaError_t FastEngine::upload_instances(const std::vector<dsmc_params> &ps,
     return cudaStreamSynchronize(stream);
 }
 
+// Captures G launches of the current kernel variant into graph_ unless an identical graph exists.
+cudaError_t FastEngine::prepare_graph(cudaStream_t stream) {
+    FastArgs a{};
+    a.inst = d_inst_;
+    a.s = slots_;
+    a.nslots = nslots_;
+    a.ctr = d_ctr_;
+    a.K = steps_per_launch;
+    const unsigned grid = static_cast<unsigned>(nslots_ / block);
+    const int key[4] = {static_cast<int>(nslots_), variant_ * 2 + (lean_ ? 1 : 0),
+                        static_cast<int>(reinterpret_cast<uintptr_t>(d_inst_) >> 8),
+                        steps_per_launch * 64 + launches_per_graph};
+    if (graph_ && graph_stream_ == stream && std::memcmp(key, graph_key_, sizeof key) == 0)
+        return cudaSuccess;
+    if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+    cudaError_t e;
+    cudaGraph_t g;
+    if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+    for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_, lean_)<<<grid, block, 0, stream>>>(a);
+    if ((e = cudaStreamEndCapture(stream, &g)) != cudaSuccess) return e;
+    e = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { graph_ = nullptr; return e; }
+    graph_stream_ = stream;
+    std::memcpy(graph_key_, key, sizeof key);
+    return cudaSuccess;
+}
+
+// One round: the captured graph (or one plain launch), then the counters copied back.
+cudaError_t FastEngine::round(cudaStream_t stream) {
+    cudaError_t e;
+    if (launches_per_graph > 1) {
+        if ((e = cudaGraphLaunch(graph_, stream)) != cudaSuccess) return e;
+        launches += launches_per_graph;
+    } else {
+        FastArgs a{};
+        a.inst = d_inst_;
+        a.s = slots_;
+        a.nslots = nslots_;
+        a.ctr = d_ctr_;
+        a.K = steps_per_launch;
+        kernel_variant(variant_, lean_)<<<static_cast<unsigned>(nslots_ / block), block, 0, stream>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        launches += 1;
+    }
+    if ((e = cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(FastCounters), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+        return e;
+    return cudaStreamSynchronize(stream);
+}
+
 cudaError_t FastEngine::drain(long long total, cudaStream_t stream) {
     cudaError_t e;
     launches = 0;
     if (total <= 0) return cudaSuccess;
-    if ((e = cudaMemsetAsync(d_ctr_, 0, sizeof(FastCounters), stream)) != cudaSuccess) return e;
+    h_ctr_->next = 0;
+    h_ctr_->finished = 0;
+    h_ctr_->total = static_cast<unsigned long long>(total);
+    h_ctr_->ninst = ninst_;
+    if ((e = cudaMemcpyAsync(d_ctr_, h_ctr_, sizeof(FastCounters), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        return e;
     if ((e = cudaMemsetAsync(slots_.inst, 0xff, nslots_ * sizeof(int), stream)) != cudaSuccess) return e;
-    FastArgs a{};
-    a.inst = d_inst_;
-    a.ninst = ninst_;
-    a.s = slots_;
-    a.nslots = nslots_;
-    a.ctr = d_ctr_;
-    a.total = total;
-    a.K = steps_per_launch;
-    const unsigned grid = static_cast<unsigned>(nslots_ / block);
-    const int key[4] = {static_cast<int>(total & 0x7fffffff), static_cast<int>(total >> 31),
-                        (ninst_ * 8 + variant_) * 2 + (lean_ ? 1 : 0),
-                        steps_per_launch * 64 + launches_per_graph};
-    const bool use_graph = launches_per_graph > 1;
-    if (use_graph && (!graph_ || graph_stream_ != stream || std::memcmp(key, graph_key_, sizeof key) != 0)) {
-        if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
-        cudaGraph_t g;
-        if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-        for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_, lean_)<<<grid, block, 0, stream>>>(a);
-        if ((e = cudaStreamEndCapture(stream, &g)) != cudaSuccess) return e;
-        e = cudaGraphInstantiate(&graph_, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) { graph_ = nullptr; return e; }
-        graph_stream_ = stream;
-        std::memcpy(graph_key_, key, sizeof key);
-    }
+    if (launches_per_graph > 1 && (e = prepare_graph(stream)) != cudaSuccess) return e;
     // Every launch advances each live particle by K steps or ends it, and every life is bounded
     // by its step caps, so the queue drains. The loop still gives up (launch-timeout status) if
     // no particle finishes for 4096 rounds, which would mean a logic error, not a long solve.
@@ -1230,17 +1266,7 @@ cudaError_t FastEngine::drain(long long total, cudaStream_t stream) {
     long long stalled = 0;
     for (;;) {
         if (stalled > 4096) return cudaErrorLaunchTimeout;
-        if (use_graph) {
-            if ((e = cudaGraphLaunch(graph_, stream)) != cudaSuccess) return e;
-            launches += launches_per_graph;
-        } else {
-            kernel_variant(variant_, lean_)<<<grid, block, 0, stream>>>(a);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
-            launches += 1;
-        }
-        if ((e = cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(FastCounters), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
-            return e;
-        if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+        if ((e = round(stream)) != cudaSuccess) return e;
         if (h_ctr_->finished >= static_cast<unsigned long long>(total)) return cudaSuccess;
         stalled = h_ctr_->finished == last ? stalled + 1 : 0;
         last = h_ctr_->finished;
@@ -1272,6 +1298,130 @@ cudaError_t FastEngine::run_batch(const std::vector<dsmc_params> &ps, const std:
     long long total = 0;
     for (long long c : counts) total += c;
     return drain(total, stream);
+}
+
+cudaError_t FastEngine::serve_open(int num_sms, int max_instances, cudaStream_t stream) {
+    if (max_instances < 1) return cudaErrorInvalidValue;
+    lean_ = false;   // a served mix may hold any kind of instance
+    cudaError_t e = ensure_slots(num_sms);
+    if (e != cudaSuccess) return e;
+    for (void *p : inst_tabs_)
+        if (p) cudaFreeAsync(p, stream);
+    inst_tabs_.assign(static_cast<size_t>(max_instances), nullptr);
+    if (max_instances > ninst_cap_) {
+        if (d_inst_) cudaFree(d_inst_);
+        d_inst_ = nullptr;
+        if ((e = cudaMalloc(&d_inst_, static_cast<size_t>(max_instances) * sizeof(FastInst))) != cudaSuccess) return e;
+        ninst_cap_ = max_instances;
+        if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+    }
+    if (!d_stats_ || stats_cap_ < max_instances) {
+        if (d_stats_) cudaFree(d_stats_);
+        d_stats_ = nullptr;
+        if ((e = cudaMalloc(&d_stats_, static_cast<size_t>(max_instances) * kStatCount * sizeof(unsigned long long))) != cudaSuccess)
+            return e;
+        stats_cap_ = max_instances;
+    }
+    if ((e = cudaMemsetAsync(d_stats_, 0, static_cast<size_t>(max_instances) * kStatCount * sizeof(unsigned long long), stream)) != cudaSuccess)
+        return e;
+    ninst_ = 0;
+    serve_total_ = 0;
+    launches = 0;
+    if ((e = cudaMemsetAsync(d_ctr_, 0, sizeof(FastCounters), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(slots_.inst, 0xff, nslots_ * sizeof(int), stream)) != cudaSuccess) return e;
+    if (launches_per_graph > 1 && (e = prepare_graph(stream)) != cudaSuccess) return e;
+    return cudaStreamSynchronize(stream);
+}
+
+namespace {
+
+// Grows the served queue to `total` work items over `ninst` instances. Grabs made while the
+// queue was empty pushed `next` past the old end without taking work (start_next returns on
+// w >= total), so those indices are handed back first.
+__global__ void publish_queue_kernel(FastCounters *c, unsigned long long old_total,
+                                     unsigned long long total, long long ninst) {
+    if (c->next > old_total) c->next = old_total;
+    c->total = total;
+    c->ninst = ninst;
+}
+
+}  // namespace
+
+cudaError_t FastEngine::serve_append(const dsmc_params &p, const DevTables &t, long long n,
+                                     int *index, cudaStream_t upload, cudaStream_t compute) {
+    if (ninst_ >= ninst_cap_ || !d_stats_) return cudaErrorMemoryAllocation;
+    if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767 || n < 0 || n > (1ll << 32)) return cudaErrorInvalidValue;
+    const size_t need = serve_table_floats(p);
+    void *d_tab = nullptr;
+    cudaError_t e = pool_ ? cudaMallocFromPoolAsync(&d_tab, need * sizeof(float), pool_, upload)
+                          : cudaMallocAsync(&d_tab, need * sizeof(float), upload);
+    if (e != cudaSuccess) return e;
+    std::vector<float> tab(need, 0.0f);
+    FastInst host;
+    DevTables tt = t;
+    tt.stats = d_stats_ + static_cast<size_t>(ninst_) * kStatCount;
+    if ((e = fast_fill_instance(p, tt, 0, n, static_cast<float *>(d_tab), need, &host, tab.data())) != cudaSuccess) {
+        cudaFreeAsync(d_tab, upload);
+        return e;
+    }
+    host.work_base = static_cast<long long>(serve_total_);
+    // The new descriptor lies beyond the instances the kernels in flight can see; it is written
+    // on the upload stream while they run, and published on the compute stream after them.
+    if ((e = cudaMemcpyAsync(d_tab, tab.data(), need * sizeof(float), cudaMemcpyHostToDevice, upload)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d_inst_ + ninst_, &host, sizeof host, cudaMemcpyHostToDevice, upload)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(upload)) != cudaSuccess) {
+        cudaFreeAsync(d_tab, upload);
+        return e;
+    }
+    inst_tabs_[static_cast<size_t>(ninst_)] = d_tab;
+    const unsigned long long old_total = serve_total_;
+    serve_total_ += static_cast<unsigned long long>(n);
+    publish_queue_kernel<<<1, 1, 0, compute>>>(d_ctr_, old_total, serve_total_, ninst_ + 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        serve_total_ = old_total;
+        return e;
+    }
+    *index = ninst_++;
+    return cudaSuccess;
+}
+
+cudaError_t FastEngine::serve_launch(cudaStream_t stream) {
+    if (launches_per_graph > 1) {
+        const cudaError_t e = cudaGraphLaunch(graph_, stream);
+        if (e == cudaSuccess) launches += launches_per_graph;
+        return e;
+    }
+    FastArgs a{};
+    a.inst = d_inst_;
+    a.s = slots_;
+    a.nslots = nslots_;
+    a.ctr = d_ctr_;
+    a.K = steps_per_launch;
+    kernel_variant(variant_, lean_)<<<static_cast<unsigned>(nslots_ / block), block, 0, stream>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) launches += 1;
+    return e;
+}
+
+void FastEngine::serve_release(int index, cudaStream_t stream) {
+    if (index < 0 || index >= static_cast<int>(inst_tabs_.size())) return;
+    if (inst_tabs_[static_cast<size_t>(index)]) cudaFreeAsync(inst_tabs_[static_cast<size_t>(index)], stream);
+    inst_tabs_[static_cast<size_t>(index)] = nullptr;
+}
+
+void FastEngine::serve_close(cudaStream_t stream) {
+    for (void *p : inst_tabs_)
+        if (p) cudaFreeAsync(p, stream);
+    inst_tabs_.clear();
+}
+
+size_t FastEngine::serve_table_floats(const dsmc_params &p) {
+    return static_cast<size_t>(p.hd + 1) + (p.ftd + 1) + 1 + 2 * static_cast<size_t>(p.ffd + 1);
+}
+
+size_t FastEngine::serve_fixed_bytes(int max_instances) const {
+    return fast_slot_bytes(nslots_) + static_cast<size_t>(max_instances) * (sizeof(FastInst) + kStatCount * 8) +
+           sizeof(FastCounters);
 }
 
 size_t fast_slot_bytes(long long nslots) {
@@ -1358,18 +1508,20 @@ cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long ns
     s.rest = reinterpret_cast<float *>(take(4));
     s.wcur = reinterpret_cast<float *>(take(4));
     cudaError_t e;
-    if ((e = cudaMemsetAsync(d_ctr, 0, sizeof(FastCounters), stream)) != cudaSuccess) return e;
+    FastCounters host{};
+    host.total = static_cast<unsigned long long>(total);
+    host.ninst = 1;
+    if ((e = cudaMemcpyAsync(d_ctr, &host, sizeof host, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(s.inst, 0xff, S * sizeof(int), stream)) != cudaSuccess) return e;
+    // the pageable source must stay valid until the copy has been made
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
     FastArgs a{};
     a.inst = static_cast<const FastInst *>(d_inst);
-    a.ninst = 1;
     a.s = s;
     a.nslots = S;
     a.ctr = static_cast<FastCounters *>(d_ctr);
-    a.total = total;
     a.K = steps_per_launch;
     const unsigned grid = static_cast<unsigned>(S / block);
-    FastCounters host{};
     unsigned long long last = 0;
     long long stalled = 0;
     for (;;) {

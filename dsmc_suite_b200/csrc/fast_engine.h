@@ -47,9 +47,13 @@ struct Slots {
     float *wcur;             // running weight (the hot loop's W between launches)
 };
 
+// Device-side queue state. `total` and `ninst` live here rather than in the kernel arguments so
+// that the host can append instances between launches of an already captured graph.
 struct FastCounters {
     unsigned long long next;      // next work index
     unsigned long long finished;  // particles whose life ended
+    unsigned long long total;     // work items in the queue (sum of the instances' particles)
+    long long ninst;              // instances in the queue
 };
 
 // Pieces of the engine for callers that supply every buffer themselves (no allocation here):
@@ -105,6 +109,37 @@ private:
                                  const std::vector<long long> &counts,
                                  const std::vector<long long> &pid_begins, cudaStream_t stream);
     cudaError_t drain(long long total, cudaStream_t stream);
+    cudaError_t prepare_graph(cudaStream_t stream);
+    cudaError_t round(cudaStream_t stream);
+
+public:
+    // Serving: an open queue that grows while it drains. serve_open resets the engine to an
+    // empty queue with room for max_instances instances. serve_append adds one instance: its
+    // boundary tables and descriptor are written on `upload` (which it synchronises), and the
+    // larger queue is published on `compute` in stream order, so kernels already in flight are
+    // not waited for; its statistics go to the engine's per-instance row `index`. serve_launch
+    // enqueues one round (the captured graph, or one launch) without waiting. serve_release
+    // frees an instance's boundary tables once all its particles have finished.
+    cudaError_t serve_open(int num_sms, int max_instances, cudaStream_t stream);
+    cudaError_t serve_append(const dsmc_params &p, const DevTables &t, long long n, int *index,
+                             cudaStream_t upload, cudaStream_t compute);
+    cudaError_t serve_launch(cudaStream_t stream);
+    void serve_release(int index, cudaStream_t stream);
+    const FastCounters *serve_counters() const { return d_ctr_; }
+    const unsigned long long *serve_stats_rows() const { return d_stats_; }
+    int serve_instances() const { return ninst_; }
+    int serve_capacity() const { return ninst_cap_; }
+    static size_t serve_table_floats(const dsmc_params &p);
+    void serve_set_pool(cudaMemPool_t pool) { pool_ = pool; }
+    void serve_close(cudaStream_t stream);   // frees every instance's boundary tables
+    size_t serve_fixed_bytes(int max_instances) const;
+
+private:
+    unsigned long long *d_stats_ = nullptr;   // [max_instances][kStatCount] (serving)
+    int stats_cap_ = 0;
+    cudaMemPool_t pool_ = nullptr;            // stream-ordered allocations (serving)
+    std::vector<void *> inst_tabs_;           // boundary tables per instance (serving)
+    unsigned long long serve_total_ = 0;
     void free_all();
 
     Slots slots_{};

@@ -223,6 +223,61 @@ int dsmc_solve_fast_noalloc(const dsmc_params *p, const dsmc_surface *surf, int6
                             void *stream);
 const char *dsmc_noalloc_last_error(void);
 
+/* ---- Batched and served solves ------------------------------------------------------------- */
+/* No counterpart in the reference, whose runners solve one problem per call                   */
+/* (src/dsmc/ballistic.c:38, src/dsmc/advanced.c:132). A server owns one GPU: a fixed set of     */
+/* resident particle slots (FAST_FP32 engine), one device work queue and a memory budget.       */
+/* Each request is a whole problem (params, surface, optional collision tables, n particles     */
+/* with ids [0, n)); its particles join the queue behind the ones already queued, and slots     */
+/* freed by ended particles take them while earlier requests are still running. A batch is a    */
+/* set of requests submitted before the first poll. Results of a request are bit-identical     */
+/* whatever else shares the queue and whatever the launch shape. Not thread-safe: one host     */
+/* thread drives a server; several servers may coexist.                                          */
+typedef struct dsmc_server dsmc_server;
+
+typedef struct dsmc_server_info {
+    int64_t submitted, completed, fetched, rejected;  /* requests */
+    int64_t active;             /* submitted and not yet complete */
+    int64_t bytes_in_use;       /* device bytes held: engine + unfetched requests */
+    int64_t bytes_budget;
+    int64_t slots;              /* resident particle slots */
+    int64_t rounds, launches;   /* rounds (graph replays) and kernel launches issued */
+    int64_t total_steps;        /* particle steps of completed requests */
+    double busy_ms;             /* device time of the rounds (CUDA events) */
+} dsmc_server_info;
+
+typedef struct dsmc_request_info {
+    int64_t n;                  /* particles */
+    int64_t ncell, nhcell;      /* density and horizon grid sizes */
+    double t_submit, t_done;    /* server clock [s] (dsmc_server_now) at admission and at the */
+                                /* poll that saw the last particle end */
+} dsmc_request_info;
+
+/* hbm_budget: device bytes the server may hold (engine slots and tables plus every admitted,  */
+/* unfetched request); max_requests: requests the queue can hold before it must drain (it     */
+/* restarts from empty whenever no request is active). */
+int dsmc_server_create(int device, int64_t hbm_budget, int max_requests, dsmc_server **out);
+int dsmc_server_destroy(dsmc_server *srv);
+const char *dsmc_server_last_error(const dsmc_server *srv);
+/* Launch shape of the engine (see dsmc_set_launch_shape); only while no request is active. */
+int dsmc_server_set_shape(dsmc_server *srv, int block, int blocks_per_sm, int steps_per_launch,
+                          int launches_per_graph);
+/* Admit one request. DSMC_ERR_BUDGET (nothing allocated) when it does not fit the budget or   */
+/* the queue is full; retry after fetching results. On success *ticket names the request.      */
+int dsmc_server_submit(dsmc_server *srv, const dsmc_params *p, const dsmc_surface *surf,
+                       const dsmc_collision *col, int64_t n, int64_t *ticket);
+/* Advance the queue: keeps up to two rounds in flight and waits for the oldest. Writes the    */
+/* tickets that completed in this call to done[0..*ndone) (at most cap; the rest are reported  */
+/* by later calls). Returns at once with *ndone = 0 when nothing is active or pending. */
+int dsmc_server_poll(dsmc_server *srv, int64_t *done, int cap, int *ndone);
+/* Copy a completed request's results to host memory (any pointer may be NULL) and free its   */
+/* device memory. DSMC_ERR_STATE while the request is still running. */
+int dsmc_server_fetch(dsmc_server *srv, int64_t ticket, uint64_t *density, uint64_t *horizon,
+                      dsmc_stats *stats, dsmc_request_info *info);
+int dsmc_server_info_get(const dsmc_server *srv, dsmc_server_info *info);
+/* Seconds since the server was created, on the clock of dsmc_request_info. */
+double dsmc_server_now(const dsmc_server *srv);
+
 #ifdef __cplusplus
 }
 #endif
