@@ -184,8 +184,9 @@ __device__ int cell_from_scratch(const FastInst &I, const float x, const float y
     track_angles(I, x, y, z, r2, td, fd);
     int ht;
     if (I.p.use_exp_grid) {
-        const double arg = I.p.alpha2 * (static_cast<double>(r) - I.p.Radii) / I.p.unih + 1.0;
-        ht = arg <= 1.0 ? 0 : static_cast<int>(log(arg) / I.p.log1p_alpha2);
+        // FP32 estimate; track_shell below settles the exact shell
+        const float arg = static_cast<float>(I.p.alpha2 / I.p.unih) * (r - static_cast<float>(I.p.Radii)) + 1.0f;
+        ht = arg <= 1.0f ? 0 : static_cast<int>(logf(arg) * static_cast<float>(1.0 / I.p.log1p_alpha2));
     } else {
         ht = static_cast<int>((static_cast<double>(r) - I.p.Radii) / I.p.unih);
     }
@@ -436,14 +437,17 @@ __device__ bool launch(const FastArgs &a, long long i, const FastInst &I, Hot &h
         const float vn = sigma * sqrtf(-2.0f * logf(1.0f - unit_open(rng.w[0])));
         const float rho = sqrtf(-2.0f * logf(1.0f - unit_open(rng.w[1])));
         float sa, ca;
-        sincosf(2.0f * kPiF * unit_open(rng.w[2]), &sa, &ca);
+        __sincosf(2.0f * kPiF * unit_open(rng.w[2]), &sa, &ca);   // argument in [0, 2 pi)
         const float t1 = rho * ca, t2 = rho * sa;
-        const float R = sqrtf(static_cast<float>(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]));
-        const float n[3] = {static_cast<float>(s[0]) / R, static_cast<float>(s[1]) / R, static_cast<float>(s[2]) / R};
+        // the event path stays short (no divisions, no FP64 square roots): unit normal and
+        // east vector by reciprocal square roots
+        const float px = h.sh[0] + h.sl[0], py = h.sh[1] + h.sl[1], pz = h.sh[2] + h.sl[2];
+        const float ir = rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz)));
+        const float n[3] = {px * ir, py * ir, pz * ir};
         float e[3] = {-n[1], n[0], 0.0f};
-        const float le = sqrtf(e[0] * e[0] + e[1] * e[1]);
-        if (le < 1e-6f) { e[0] = 1.0f; e[1] = 0.0f; }
-        else { e[0] /= le; e[1] /= le; }
+        const float le2 = fmaf(e[0], e[0], e[1] * e[1]);
+        if (le2 < 1e-12f) { e[0] = 1.0f; e[1] = 0.0f; }
+        else { const float il = rsqrtf(le2); e[0] *= il; e[1] *= il; }
         const float nt[3] = {n[1] * e[2] - n[2] * e[1], n[2] * e[0] - n[0] * e[2], n[0] * e[1] - n[1] * e[0]};
         const float omega = p.P > 0.0 ? static_cast<float>(2.0 * kPi / p.P) : 0.0f;
         const float rot[3] = {omega * static_cast<float>(s[1]), -omega * static_cast<float>(s[0]), 0.0f};
@@ -572,19 +576,25 @@ __device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &loc
         }
         return 0;
     }
-    double s[3];
-    get_pos(h, s);
-    const double R = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
-    double n[3] = {s[0] / R, s[1] / R, s[2] / R};
-    if (n[0] * p.sun[0] + n[1] * p.sun[1] + n[2] * p.sun[2] <= 0.0) {
-        angles_of(h, thi, fi);
-        ref_index(thi, fi, p.ftd, p.ffd, td, fd);
+    // FP32 normal; the landing cell of a night-side freeze-out by comparison walks from the
+    // last cell (the upper-inclusive cells of grid_spherical_to_index without asin or atan2)
+    const float x = h.sh[0] + h.sl[0], y = h.sh[1] + h.sl[1], z = h.sh[2] + h.sl[2];
+    const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+    const float ir = rsqrtf(r2);
+    const float n[3] = {x * ir, y * ir, z * ir};
+    if (fmaf(n[0], static_cast<float>(p.sun[0]), fmaf(n[1], static_cast<float>(p.sun[1]),
+                                                      n[2] * static_cast<float>(p.sun[2]))) <= 0.0f) {
+        td = (h.cell >> 8) & 0xff;
+        fd = h.cell & 0xff;
+        track_angles(I, x, y, z, r2, td, fd);
         horizon_add(I, td, fd, weight(I, h));
         return DSMC_FATE_FROZEN;
     }
-    for (int k = 0; k < 3; k++) s[k] = n[k] * p.Radii;
+    // day side: re-emission from the surface point below the landing point
+    const double nd[3] = {n[0], n[1], n[2]};
+    const double s[3] = {nd[0] * p.Radii, nd[1] * p.Radii, nd[2] * p.Radii};
     set_pos(h, s);
-    local_T = static_cast<float>(I.t.face_T[locate_face(I.t, n)]);
+    local_T = static_cast<float>(I.t.face_T[locate_face(I.t, nd)]);
     return 0;
 }
 
@@ -662,7 +672,7 @@ __device__ void collide(const FastArgs &a, long long i, const FastInst &I, Hot &
     }
     a.s.evt[i] = rng.event;
     a.s.ncol[i] += 1;
-    if (col_p >= 0.0) h.pthr = static_cast<float>(-log1p(-col_p));
+    if (col_p >= 0.0) h.pthr = -log1pf(-static_cast<float>(col_p));
     set_vel(h, v);
     h.pcol = 0.0f;
 }
@@ -743,19 +753,23 @@ __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, St
             const double *fv = I.t.face_verts + 9 * f;
             double q[3];
             for (int k = 0; k < 3; k++) q[k] = fv[k] + u1 * (fv[3 + k] - fv[k]) + u2 * (fv[6 + k] - fv[k]);
-            const double lq = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
-            for (int k = 0; k < 3; k++) s[k] = q[k] * (p.Radii / lq);
+            // |q|^-1 from the FP32 estimate and one Newton step in FP64 (relative error ~1e-14)
+            const double q2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+            double iq = rsqrtf(static_cast<float>(q2));
+            iq = iq * (1.5 - 0.5 * q2 * iq * iq);
+            for (int k = 0; k < 3; k++) s[k] = q[k] * (p.Radii * iq);
             local_T = static_cast<float>(I.t.face_T[f]);
+            thi = fi = 0.0f;   // the config model's launch does not use the angles
         }
         a.s.pid[i] = pid;
         a.s.evt[i] = rng.event;
         a.s.ncol[i] = 0;
         a.s.rest[i] = 0.0f;
-        h.pthr = static_cast<float>(-log1p(-col_p));
+        h.pthr = p.runner == DSMC_RUNNER_ADVANCED ? -log1pf(-static_cast<float>(col_p)) : 0.0f;
         set_pos(h, s);
-        if (p.model != DSMC_MODEL_REFERENCE) angles_of(h, thi, fi);
         const long long slot = static_cast<long long>(pid) - I.t.out_base;
         if (I.t.ttime && slot >= 0 && slot < I.t.out_cap) {
+            if (p.model != DSMC_MODEL_REFERENCE) angles_of(h, thi, fi);
             I.t.ttime[slot] = thi;
             if (p.runner == DSMC_RUNNER_ADVANCED || p.model != DSMC_MODEL_REFERENCE) {
                 I.t.ttime[5 * I.t.out_cap + slot] = fi;
