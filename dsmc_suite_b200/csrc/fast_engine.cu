@@ -1010,6 +1010,8 @@ FastEngine::~FastEngine() { free_all(); }
 void FastEngine::free_all() {
     if (graph_) cudaGraphExecDestroy(graph_);
     graph_ = nullptr;
+    if (graph_lean_) cudaGraphExecDestroy(graph_lean_);
+    graph_lean_ = nullptr;
     if (slot_mem_) cudaFree(slot_mem_);
     slot_mem_ = nullptr;
     if (d_inst_) cudaFree(d_inst_);
@@ -1082,6 +1084,7 @@ cudaError_t FastEngine::ensure_slots(int num_sms) {
     const long long want = static_cast<long long>(num_sms) * per_sm * block;
     if (slot_mem_ && nslots_ == want) return cudaSuccess;
     if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+    if (graph_lean_) { cudaGraphExecDestroy(graph_lean_); graph_lean_ = nullptr; }
     if (slot_mem_) { cudaFree(slot_mem_); slot_mem_ = nullptr; }
     const long long S = want;
     // 4-byte fields: inst pid evt (3) + 15 vector floats + w0 nday steps hop cell run_cell
@@ -1213,6 +1216,21 @@ cudaError_t FastEngine::upload_instances(const std::vector<dsmc_params> &ps,
 
 // Captures G launches of the current kernel variant into graph_ unless an identical graph exists.
 cudaError_t FastEngine::prepare_graph(cudaStream_t stream) {
+    const int key[4] = {static_cast<int>(nslots_), variant_ * 2 + (lean_ ? 1 : 0),
+                        static_cast<int>(reinterpret_cast<uintptr_t>(d_inst_) >> 8),
+                        steps_per_launch * 64 + launches_per_graph};
+    if (graph_ && graph_stream_ == stream && std::memcmp(key, graph_key_, sizeof key) == 0)
+        return cudaSuccess;
+    if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+    const cudaError_t e = capture(stream, lean_, &graph_);
+    if (e != cudaSuccess) return e;
+    graph_stream_ = stream;
+    std::memcpy(graph_key_, key, sizeof key);
+    return cudaSuccess;
+}
+
+// G launches of the current variant (lean or general loop) captured as one graph.
+cudaError_t FastEngine::capture(cudaStream_t stream, bool lean, cudaGraphExec_t *out) {
     FastArgs a{};
     a.inst = d_inst_;
     a.s = slots_;
@@ -1220,23 +1238,16 @@ cudaError_t FastEngine::prepare_graph(cudaStream_t stream) {
     a.ctr = d_ctr_;
     a.K = steps_per_launch;
     const unsigned grid = static_cast<unsigned>(nslots_ / block);
-    const int key[4] = {static_cast<int>(nslots_), variant_ * 2 + (lean_ ? 1 : 0),
-                        static_cast<int>(reinterpret_cast<uintptr_t>(d_inst_) >> 8),
-                        steps_per_launch * 64 + launches_per_graph};
-    if (graph_ && graph_stream_ == stream && std::memcmp(key, graph_key_, sizeof key) == 0)
-        return cudaSuccess;
-    if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
     cudaError_t e;
     cudaGraph_t g;
+    *out = nullptr;
     if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-    for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_, lean_)<<<grid, block, 0, stream>>>(a);
+    for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_, lean)<<<grid, block, 0, stream>>>(a);
     if ((e = cudaStreamEndCapture(stream, &g)) != cudaSuccess) return e;
-    e = cudaGraphInstantiate(&graph_, g, 0);
+    e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) { graph_ = nullptr; return e; }
-    graph_stream_ = stream;
-    std::memcpy(graph_key_, key, sizeof key);
-    return cudaSuccess;
+    if (e != cudaSuccess) *out = nullptr;
+    return e;
 }
 
 // One round: the captured graph (or one plain launch), then the counters copied back.
@@ -1344,7 +1355,14 @@ cudaError_t FastEngine::serve_open(int num_sms, int max_instances, cudaStream_t 
     if ((e = cudaMemsetAsync(d_ctr_, 0, sizeof(FastCounters), stream)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(slots_.inst, 0xff, nslots_ * sizeof(int), stream)) != cudaSuccess) return e;
     if (launches_per_graph > 1 && (e = prepare_graph(stream)) != cudaSuccess) return e;
+    // the lean loop over the same slots, for rounds in which every queued instance qualifies
+    if (graph_lean_) { cudaGraphExecDestroy(graph_lean_); graph_lean_ = nullptr; }
+    if (launches_per_graph > 1 && (e = capture(stream, true, &graph_lean_)) != cudaSuccess) return e;
     return cudaStreamSynchronize(stream);
+}
+
+bool FastEngine::lean_eligible(const dsmc_params &p, const DevTables &t) {
+    return all_lean({p}, {t});
 }
 
 namespace {
@@ -1399,9 +1417,9 @@ cudaError_t FastEngine::serve_append(const dsmc_params &p, const DevTables &t, l
     return cudaSuccess;
 }
 
-cudaError_t FastEngine::serve_launch(cudaStream_t stream) {
+cudaError_t FastEngine::serve_launch(cudaStream_t stream, bool lean) {
     if (launches_per_graph > 1) {
-        const cudaError_t e = cudaGraphLaunch(graph_, stream);
+        const cudaError_t e = cudaGraphLaunch(lean ? graph_lean_ : graph_, stream);
         if (e == cudaSuccess) launches += launches_per_graph;
         return e;
     }
@@ -1411,7 +1429,7 @@ cudaError_t FastEngine::serve_launch(cudaStream_t stream) {
     a.nslots = nslots_;
     a.ctr = d_ctr_;
     a.K = steps_per_launch;
-    kernel_variant(variant_, lean_)<<<static_cast<unsigned>(nslots_ / block), block, 0, stream>>>(a);
+    kernel_variant(variant_, lean)<<<static_cast<unsigned>(nslots_ / block), block, 0, stream>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) launches += 1;
     return e;

@@ -35,6 +35,7 @@ struct Request {
     size_t bytes = 0;                       // charged against the budget
     unsigned long long stats[dsmc::kStatCount] = {};
     double t_submit = 0.0, t_done = 0.0;
+    bool lean = false;                      // may run in the engine's lean loop
     enum State { kActive, kDone, kFetched } state = kActive;
 };
 
@@ -65,6 +66,7 @@ struct dsmc_server {
     double busy_ms = 0.0;
     unsigned long long last_finished = 0;
     long long stalled = 0;
+    long long general_active = 0;                   // active requests the lean loop cannot run
     char err[512] = {0};
 };
 
@@ -112,7 +114,9 @@ int launch_round(dsmc_server *s) {
     R.lo = s->reqs[static_cast<size_t>(s->active.front())]->inst;
     R.hi = s->engine.serve_instances();
     cudaError_t e = cudaEventRecord(R.start, s->compute);
-    if (e == cudaSuccess) e = s->engine.serve_launch(s->compute);
+    // Rounds run the lean loop while every queued request qualifies for it (same results, fewer
+    // registers and branches); a request published after this launch is not seen by it.
+    if (e == cudaSuccess) e = s->engine.serve_launch(s->compute, s->general_active == 0);
     if (e == cudaSuccess) s->nlaunches += std::max(1, s->engine.launches_per_graph);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(R.snap, s->engine.serve_counters(), sizeof(dsmc::FastCounters),
@@ -155,6 +159,7 @@ int retire_round(dsmc_server *s) {
         if (done) {
             q.state = Request::kDone;
             q.t_done = t;
+            if (!q.lean) s->general_active--;
             s->completed++;
             s->total_steps += static_cast<long long>(q.stats[dsmc::kStatSteps]);
             s->done_queue.push_back(tk);
@@ -333,6 +338,8 @@ int dsmc_server_submit(dsmc_server *s, const dsmc_params *p, const dsmc_surface 
         e = s->engine.serve_append(*p, q->prob->t, n, &q->inst, s->upload, s->compute);
         if (e != cudaSuccess) return cuda_fail(s, "appending to the work queue", e);
         s->active.push_back(tk);
+        q->lean = dsmc::FastEngine::lean_eligible(*p, q->prob->t);
+        if (!q->lean) s->general_active++;
     } else {
         q->state = Request::kDone;
         q->t_done = q->t_submit;
