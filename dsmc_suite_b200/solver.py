@@ -44,6 +44,17 @@ class Context:
     def _check(self, status: int, where: str) -> None:
         N.check(status, where, self.h)
 
+    def set_launch_shape(self, block: int, blocks_per_sm: int, steps_per_launch: int,
+                         launches_per_graph: int) -> None:
+        self._check(self._lib.dsmc_set_launch_shape(self.h, block, blocks_per_sm, steps_per_launch,
+                                                    launches_per_graph), "set_launch_shape")
+
+    def launch_info(self) -> tuple[int, int]:
+        """(kernel launches of the last run, resident slots) of the FAST paths."""
+        la, ns = C.c_int64(), C.c_int64()
+        self._check(self._lib.dsmc_get_launch_info(self.h, C.byref(la), C.byref(ns)), "launch_info")
+        return la.value, ns.value
+
     def set_stream(self, stream_ptr: int | None) -> None:
         self._check(self._lib.dsmc_ctx_set_stream(self.h, C.c_void_p(stream_ptr or 0)), "set_stream")
 

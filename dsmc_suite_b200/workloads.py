@@ -173,17 +173,28 @@ def two_phase_tables(ctx, p1: N.Params, surf: N.SurfaceInputs, n1: int, rate: fl
     return col, nden
 
 
+# Total water production of the collisional problems [molecules/s]: Ceres' observed ~6 kg/s.
+# The Antoine sublimation flux of a fully icy surface at these temperatures would be ~1e33/s, a
+# near-surface mean free path below a millimetre, where a test-particle scheme (collisions against
+# a fixed background) no longer applies; the flux sets where particles start, this rate sets how
+# many molecules each test particle stands for, hence the background density of phase 2.
+PRODUCTION_RATE = 2.0e26
+
+
 def collisional_problem(ctx, name: str, R: float, GM: float, hd: int, seed: int, sun, T_ss: float,
-                        n1: int, n2: int, path: int = N.PATH_FAST_FP32) -> Problem:
-    """A config-model collisional problem: Antoine-flux source on the T map, phase-1 tables."""
+                        n1: int, n2: int, path: int = N.PATH_FAST_FP32,
+                        production_rate: float | None = PRODUCTION_RATE) -> Problem:
+    """A config-model collisional problem: Antoine-flux source on the T map, phase-1 tables.
+    production_rate None keeps the full Antoine rate of an all-ice surface."""
     surf, rate_r2 = config_surface(sun, T_ss, flux_weighted=True)
-    rate = rate_r2 * R * R
+    antoine_rate = rate_r2 * R * R
+    rate = antoine_rate if production_rate is None else production_rate
     p = N.params_config(N.RUNNER_ADVANCED, R, GM, hd, seed)
     p.sun[0], p.sun[1], p.sun[2] = sun
     p.cross_section = math.pi * D_H2O * D_H2O
     col, nden = two_phase_tables(ctx, p, surf, n1, rate, path=path)
-    return Problem(name, p, surf, n2, col, meta={"rate": rate, "n_phase1": n1,
-                                                   "max_n_bg": float(nden.max())})
+    return Problem(name, p, surf, n2, col, meta={"rate": rate, "antoine_rate": antoine_rate,
+                                                   "n_phase1": n1, "max_n_bg": float(nden.max())})
 
 
 def served_stream(ctx, rate_hz: float, seconds: float, seed: int = 20261203,
