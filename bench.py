@@ -268,11 +268,19 @@ def run_batch_mode(a):
     torch.cuda.set_device(local)
     probs = W.batch_instances(SEED, 64)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    srv = Server(local, hbm_budget=int(a.budget_gb * 1e9), max_requests=4096)
     if a.shape:
         shape = [int(v) for v in a.shape.split(",")]
-        srv.set_shape(*shape)
-        BATCH_CONFIG["launch_shape"] = shape
+    else:
+        # autotuned on a 5 % copy of the batch (untimed)
+        from dsmc_suite_b200 import autotune
+        tuned = autotune.tune(probs, local, scale=0.05)
+        shape = tuned["shape"]
+        BATCH_CONFIG["autotune"] = {"candidates": len(tuned["trials"]), "sample_scale": 0.05,
+                                    "best_sample_rate": tuned["rate"],
+                                    "worst_sample_rate": min(t["rate"] for t in tuned["trials"])}
+    srv = Server(local, hbm_budget=int(a.budget_gb * 1e9), max_requests=4096)
+    srv.set_shape(*shape)
+    BATCH_CONFIG["launch_shape"] = list(shape)
 
     def step():
         i0 = srv.info()
@@ -415,7 +423,7 @@ def run_collisional_mode(a):
     events; the plain FP64 path solves the same phase 2 once for the ratio and the density
     relative L2."""
     import torch
-    from dsmc_suite_b200 import _native as N, Context
+    from dsmc_suite_b200 import _native as N, Context, shard
     from dsmc_suite_b200 import workloads as W
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if int(os.environ.get("RANK", "0")) != 0:
@@ -500,7 +508,7 @@ def main():
     import torch
     import torch.distributed as dist
     from datetime import timedelta
-    from dsmc_suite_b200 import _native as N, Context
+    from dsmc_suite_b200 import _native as N, Context, shard
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -517,7 +525,7 @@ def main():
     ctx.set_stream(stream.cuda_stream)
     p, S = config_problem(N)
     n = int(a.particles)
-    pid0 = rank * n
+    pid0, _ = shard.particle_range(rank, world, n)   # weak scaling: disjoint id shards
     ctx.setup(p, S)
     if a.shape:
         shape = [int(v) for v in a.shape.split(",")]

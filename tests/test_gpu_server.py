@@ -155,3 +155,16 @@ def test_server_edge_cases(N, surf):
         with pytest.raises(N.DsmcError):
             srv.submit(p, surf, -1)
         assert srv.info()["active"] == 0
+
+
+def test_autotune_picks_the_fastest_candidate_and_caches_it(N, surf, tmp_path):
+    from dsmc_suite_b200 import autotune
+    from dsmc_suite_b200.workloads import batch_instances
+    probs = batch_instances(seed=5, count=4)
+    cands = [(128, 0, 512, 2), (128, 0, 2048, 4)]
+    cache = tmp_path / "tune.json"
+    r = autotune.tune(probs, 0, scale=0.01, candidates=cands, cache=cache)
+    assert tuple(r["shape"]) in cands and len(r["trials"]) == 2
+    assert r["rate"] == max(t["rate"] for t in r["trials"]) > 0
+    assert autotune.tune(probs, 0, scale=0.01, candidates=cands, cache=cache) == \
+        __import__("json").loads(cache.read_text())[next(iter(__import__("json").loads(cache.read_text())))]
