@@ -806,11 +806,14 @@ enum Flag { kRef = 1, kSkipFirst = 2, kCollide = 4, kHist = 8 };
 
 // kMaxThreads x kMinBlocks: the register budget the allocation must respect (65536 registers
 // per SM shared by kMinBlocks blocks of kMaxThreads). The launch shape picks the variant.
-// kLean: every instance of the launch is a config-model ballistic problem without speed
-// histograms whose hop cap is not below its life cap, so the reference-model, collision and
-// histogram branches and the per-hop step counter drop out of the loop.
-template <int kMaxThreads, int kMinBlocks, bool kLean>
+// kMode 0: the general loop. kMode 1 (lean): every instance of the launch is a config-model
+// problem without speed histograms whose hop cap is not below its life cap and that has no
+// collisions, so the reference-model, collision and histogram branches and the per-hop step
+// counter drop out of the loop. kMode 2: the same, with the collision branch kept (config-model
+// collisional instances).
+template <int kMaxThreads, int kMinBlocks, int kMode>
 __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const FastArgs a) {
+    constexpr bool kLean = kMode != 0;
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     Hot h;
     load_hot(a.s, i, a.nslots, h);
@@ -903,7 +906,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
             }
             if (kLean || !((flags & kSkipFirst) && ii == 0)) {
                 bool collided = false;
-                if (!kLean && (flags & kCollide) && h.nsig > 0.0f) {
+                if ((kMode == 0 ? (flags & kCollide) != 0 : kMode == 2) && h.nsig > 0.0f) {
                     h.pcol = fmaf(sqrtf(fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2]))), h.nsig, h.pcol);
                     if (h.pcol > h.pthr) {
                         const int ht = h.cell >> 16, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
@@ -1010,8 +1013,10 @@ FastEngine::~FastEngine() { free_all(); }
 void FastEngine::free_all() {
     if (graph_) cudaGraphExecDestroy(graph_);
     graph_ = nullptr;
-    if (graph_lean_) cudaGraphExecDestroy(graph_lean_);
-    graph_lean_ = nullptr;
+    for (cudaGraphExec_t &g : graph_mode_) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
     if (slot_mem_) cudaFree(slot_mem_);
     slot_mem_ = nullptr;
     if (d_inst_) cudaFree(d_inst_);
@@ -1036,47 +1041,60 @@ namespace {
 
 // Register budgets of fast_kernel: 0: 256 x 2 (128 registers a thread), 1: 256 x 3 (80),
 // 2: 128 x 3 (168), 3: 128 x 2 (255), 4: 128 x 4 (128).
-// The lean loop exists for budgets 0, 2 and 4.
-void (*kernel_variant(int variant, bool lean))(FastArgs) {
+// The lean loops (modes 1 and 2) exist for budgets 0, 2 and 4; elsewhere the general loop runs.
+template <int kT, int kB>
+void (*by_mode(int mode))(FastArgs) {
+    return mode == 2 ? fast_kernel<kT, kB, 2> : mode == 1 ? fast_kernel<kT, kB, 1> : fast_kernel<kT, kB, 0>;
+}
+
+void (*kernel_variant(int variant, int mode))(FastArgs) {
     switch (variant) {
-        case 1: return fast_kernel<256, 3, false>;
-        case 2: return lean ? fast_kernel<128, 3, true> : fast_kernel<128, 3, false>;
-        case 3: return fast_kernel<128, 2, false>;
-        case 4: return lean ? fast_kernel<128, 4, true> : fast_kernel<128, 4, false>;
-        default: return lean ? fast_kernel<256, 2, true> : fast_kernel<256, 2, false>;
+        case 1: return fast_kernel<256, 3, 0>;
+        case 2: return by_mode<128, 3>(mode);
+        case 3: return fast_kernel<128, 2, 0>;
+        case 4: return by_mode<128, 4>(mode);
+        default: return by_mode<256, 2>(mode);
     }
 }
 
 // Variant for a launch shape: blocks_per_sm names the register budget. The default (0) is the
 // fastest measured on B200: the lean loop fits 128 registers without spills (16 warps per SM),
 // the general loop needs 168 (12 warps per SM) to avoid them.
-int pick_variant(int block, int blocks_per_sm, bool lean) {
+int pick_variant(int block, int blocks_per_sm, int mode) {
     if (block > 128) return blocks_per_sm >= 3 ? 1 : 0;
     if (blocks_per_sm == 2) return 3;
     if (blocks_per_sm == 3) return 2;
     if (blocks_per_sm == 4) return 4;
-    return lean ? 4 : 2;
+    return mode == 1 ? 4 : 2;   // the collision loop (mode 2) fits 168 registers without spills
 }
 
-// Whether every instance qualifies for the lean loop (see fast_kernel).
-bool all_lean(const std::vector<dsmc_params> &ps, const std::vector<DevTables> &ts) {
+// Loop mode of one instance (see fast_kernel): 1 lean, 2 lean with collisions, 0 general.
+int instance_mode(const dsmc_params &p, const DevTables &t) {
+    if (p.model != DSMC_MODEL_CONFIG || p.skip_first_deposit || (t.speed_hist && p.n_speed_bins > 0) ||
+        p.life_step_cap <= 0 || p.hop_step_cap < p.life_step_cap)
+        return 0;
+    return p.runner == DSMC_RUNNER_ADVANCED && t.n_bg ? 2 : 1;
+}
+
+// The loop that can run every instance of a launch: general if any needs it, else lean with
+// collisions if any collides, else lean.
+int launch_mode(const std::vector<dsmc_params> &ps, const std::vector<DevTables> &ts) {
+    int m = 1;
     for (size_t k = 0; k < ps.size(); k++) {
-        const dsmc_params &p = ps[k];
-        if (p.model != DSMC_MODEL_CONFIG || p.runner != DSMC_RUNNER_BALLISTIC ||
-            p.skip_first_deposit || (ts[k].speed_hist && p.n_speed_bins > 0) ||
-            p.life_step_cap <= 0 || p.hop_step_cap < p.life_step_cap)
-            return false;
+        const int mk = instance_mode(ps[k], ts[k]);
+        if (mk == 0) return 0;
+        m = std::max(m, mk);
     }
-    return true;
+    return m;
 }
 
 }  // namespace
 
 cudaError_t FastEngine::ensure_slots(int num_sms) {
     // one wave: as many blocks per SM as can be resident together
-    variant_ = pick_variant(block, blocks_per_sm, lean_);
+    variant_ = pick_variant(block, blocks_per_sm, mode_);
     int resident = 0;
-    cudaError_t e0 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel_variant(variant_, lean_), block, 0);
+    cudaError_t e0 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel_variant(variant_, mode_), block, 0);
     if (e0 != cudaSuccess) return e0;
     if (resident < 1) return cudaErrorInvalidConfiguration;
     const int per_sm = (blocks_per_sm > resident || blocks_per_sm < 1) ? resident : blocks_per_sm;
@@ -1084,7 +1102,8 @@ cudaError_t FastEngine::ensure_slots(int num_sms) {
     const long long want = static_cast<long long>(num_sms) * per_sm * block;
     if (slot_mem_ && nslots_ == want) return cudaSuccess;
     if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
-    if (graph_lean_) { cudaGraphExecDestroy(graph_lean_); graph_lean_ = nullptr; }
+    for (cudaGraphExec_t &g : graph_mode_)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (slot_mem_) { cudaFree(slot_mem_); slot_mem_ = nullptr; }
     const long long S = want;
     // 4-byte fields: inst pid evt (3) + 15 vector floats + w0 nday steps hop cell run_cell
@@ -1216,13 +1235,13 @@ cudaError_t FastEngine::upload_instances(const std::vector<dsmc_params> &ps,
 
 // Captures G launches of the current kernel variant into graph_ unless an identical graph exists.
 cudaError_t FastEngine::prepare_graph(cudaStream_t stream) {
-    const int key[4] = {static_cast<int>(nslots_), variant_ * 2 + (lean_ ? 1 : 0),
+    const int key[4] = {static_cast<int>(nslots_), variant_ * 4 + mode_,
                         static_cast<int>(reinterpret_cast<uintptr_t>(d_inst_) >> 8),
                         steps_per_launch * 64 + launches_per_graph};
     if (graph_ && graph_stream_ == stream && std::memcmp(key, graph_key_, sizeof key) == 0)
         return cudaSuccess;
     if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
-    const cudaError_t e = capture(stream, lean_, &graph_);
+    const cudaError_t e = capture(stream, mode_, &graph_);
     if (e != cudaSuccess) return e;
     graph_stream_ = stream;
     std::memcpy(graph_key_, key, sizeof key);
@@ -1230,7 +1249,7 @@ cudaError_t FastEngine::prepare_graph(cudaStream_t stream) {
 }
 
 // G launches of the current variant (lean or general loop) captured as one graph.
-cudaError_t FastEngine::capture(cudaStream_t stream, bool lean, cudaGraphExec_t *out) {
+cudaError_t FastEngine::capture(cudaStream_t stream, int mode, cudaGraphExec_t *out) {
     FastArgs a{};
     a.inst = d_inst_;
     a.s = slots_;
@@ -1242,7 +1261,7 @@ cudaError_t FastEngine::capture(cudaStream_t stream, bool lean, cudaGraphExec_t 
     cudaGraph_t g;
     *out = nullptr;
     if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-    for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_, lean)<<<grid, block, 0, stream>>>(a);
+    for (int k = 0; k < launches_per_graph; k++) kernel_variant(variant_, mode)<<<grid, block, 0, stream>>>(a);
     if ((e = cudaStreamEndCapture(stream, &g)) != cudaSuccess) return e;
     e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
@@ -1263,7 +1282,7 @@ cudaError_t FastEngine::round(cudaStream_t stream) {
         a.nslots = nslots_;
         a.ctr = d_ctr_;
         a.K = steps_per_launch;
-        kernel_variant(variant_, lean_)<<<static_cast<unsigned>(nslots_ / block), block, 0, stream>>>(a);
+        kernel_variant(variant_, mode_)<<<static_cast<unsigned>(nslots_ / block), block, 0, stream>>>(a);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         launches += 1;
     }
@@ -1302,7 +1321,7 @@ cudaError_t FastEngine::run(const dsmc_params &p, const DevTables &t, bool fp64,
                             long long n, int num_sms, cudaStream_t stream) {
     if (fp64) return cudaErrorNotSupported;
     if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767) return cudaErrorInvalidValue;
-    lean_ = all_lean({p}, {t});
+    mode_ = launch_mode({p}, {t});
     cudaError_t e = ensure_slots(num_sms);
     if (e != cudaSuccess) return e;
     e = upload_instances({p}, {t}, {n}, {pid_begin}, stream);
@@ -1314,7 +1333,7 @@ cudaError_t FastEngine::run_batch(const std::vector<dsmc_params> &ps, const std:
                                   const std::vector<long long> &counts, int num_sms, cudaStream_t stream) {
     for (const auto &p : ps)
         if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767) return cudaErrorInvalidValue;
-    lean_ = all_lean(ps, ts);
+    mode_ = launch_mode(ps, ts);
     cudaError_t e = ensure_slots(num_sms);
     if (e != cudaSuccess) return e;
     std::vector<long long> pid0(ps.size(), 0);
@@ -1327,7 +1346,7 @@ cudaError_t FastEngine::run_batch(const std::vector<dsmc_params> &ps, const std:
 
 cudaError_t FastEngine::serve_open(int num_sms, int max_instances, cudaStream_t stream) {
     if (max_instances < 1) return cudaErrorInvalidValue;
-    lean_ = false;   // a served mix may hold any kind of instance
+    mode_ = 0;   // the slots are sized for the general loop; every round picks its own loop
     cudaError_t e = ensure_slots(num_sms);
     if (e != cudaSuccess) return e;
     for (void *p : inst_tabs_)
@@ -1355,15 +1374,15 @@ cudaError_t FastEngine::serve_open(int num_sms, int max_instances, cudaStream_t 
     if ((e = cudaMemsetAsync(d_ctr_, 0, sizeof(FastCounters), stream)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(slots_.inst, 0xff, nslots_ * sizeof(int), stream)) != cudaSuccess) return e;
     if (launches_per_graph > 1 && (e = prepare_graph(stream)) != cudaSuccess) return e;
-    // the lean loop over the same slots, for rounds in which every queued instance qualifies
-    if (graph_lean_) { cudaGraphExecDestroy(graph_lean_); graph_lean_ = nullptr; }
-    if (launches_per_graph > 1 && (e = capture(stream, true, &graph_lean_)) != cudaSuccess) return e;
+    // the lean loops over the same slots, for rounds in which every queued instance qualifies
+    for (int m = 1; m <= 2; m++) {
+        if (graph_mode_[m]) { cudaGraphExecDestroy(graph_mode_[m]); graph_mode_[m] = nullptr; }
+        if (launches_per_graph > 1 && (e = capture(stream, m, &graph_mode_[m])) != cudaSuccess) return e;
+    }
     return cudaStreamSynchronize(stream);
 }
 
-bool FastEngine::lean_eligible(const dsmc_params &p, const DevTables &t) {
-    return all_lean({p}, {t});
-}
+int FastEngine::loop_mode(const dsmc_params &p, const DevTables &t) { return instance_mode(p, t); }
 
 namespace {
 
@@ -1417,9 +1436,9 @@ cudaError_t FastEngine::serve_append(const dsmc_params &p, const DevTables &t, l
     return cudaSuccess;
 }
 
-cudaError_t FastEngine::serve_launch(cudaStream_t stream, bool lean) {
+cudaError_t FastEngine::serve_launch(cudaStream_t stream, int mode) {
     if (launches_per_graph > 1) {
-        const cudaError_t e = cudaGraphLaunch(lean ? graph_lean_ : graph_, stream);
+        const cudaError_t e = cudaGraphLaunch(mode ? graph_mode_[mode] : graph_, stream);
         if (e == cudaSuccess) launches += launches_per_graph;
         return e;
     }
@@ -1429,7 +1448,7 @@ cudaError_t FastEngine::serve_launch(cudaStream_t stream, bool lean) {
     a.nslots = nslots_;
     a.ctr = d_ctr_;
     a.K = steps_per_launch;
-    kernel_variant(variant_, lean)<<<static_cast<unsigned>(nslots_ / block), block, 0, stream>>>(a);
+    kernel_variant(variant_, mode)<<<static_cast<unsigned>(nslots_ / block), block, 0, stream>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) launches += 1;
     return e;
@@ -1558,7 +1577,7 @@ cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long ns
     long long stalled = 0;
     for (;;) {
         if (stalled > 4096) return cudaErrorLaunchTimeout;
-        fast_kernel<256, 2, false><<<grid, block, 0, stream>>>(a);
+        fast_kernel<256, 2, 0><<<grid, block, 0, stream>>>(a);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         *launches += 1;
         if ((e = cudaMemcpyAsync(&host, d_ctr, sizeof host, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)

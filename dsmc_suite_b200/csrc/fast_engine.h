@@ -110,7 +110,7 @@ private:
                                  const std::vector<long long> &pid_begins, cudaStream_t stream);
     cudaError_t drain(long long total, cudaStream_t stream);
     cudaError_t prepare_graph(cudaStream_t stream);
-    cudaError_t capture(cudaStream_t stream, bool lean, cudaGraphExec_t *out);
+    cudaError_t capture(cudaStream_t stream, int mode, cudaGraphExec_t *out);
     cudaError_t round(cudaStream_t stream);
 
 public:
@@ -124,10 +124,11 @@ public:
     cudaError_t serve_open(int num_sms, int max_instances, cudaStream_t stream);
     cudaError_t serve_append(const dsmc_params &p, const DevTables &t, long long n, int *index,
                              cudaStream_t upload, cudaStream_t compute);
-    cudaError_t serve_launch(cudaStream_t stream, bool lean);
-    // Whether an instance may run in the lean loop (config model, ballistic, no speed histogram,
-    // hop cap not below the life cap); the lean and general loops give identical results for it.
-    static bool lean_eligible(const dsmc_params &p, const DevTables &t);
+    cudaError_t serve_launch(cudaStream_t stream, int mode);
+    // Loop an instance may run in: 1 lean (config model, ballistic, no speed histogram, hop cap
+    // not below the life cap), 2 lean with collisions (the same, collisional), 0 general only.
+    // Every loop that can run an instance gives it identical results.
+    static int loop_mode(const dsmc_params &p, const DevTables &t);
     void serve_release(int index, cudaStream_t stream);
     const FastCounters *serve_counters() const { return d_ctr_; }
     const unsigned long long *serve_stats_rows() const { return d_stats_; }
@@ -157,12 +158,12 @@ private:
     FastCounters *d_ctr_ = nullptr;
     FastCounters *h_ctr_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
-    cudaGraphExec_t graph_lean_ = nullptr;   // serving: the lean loop over the same slots
+    cudaGraphExec_t graph_mode_[3] = {nullptr, nullptr, nullptr};   // serving: lean loops 1, 2
     cudaStream_t graph_stream_ = nullptr;
     int graph_key_[4] = {0, 0, 0, 0};
     bool nslots_want_changed_ = false;
     int variant_ = 2;
-    bool lean_ = false;
+    int mode_ = 0;   // loop of run / run_batch launches (see fast_kernel)
 };
 
 }  // namespace dsmc

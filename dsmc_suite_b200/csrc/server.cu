@@ -35,7 +35,7 @@ struct Request {
     size_t bytes = 0;                       // charged against the budget
     unsigned long long stats[dsmc::kStatCount] = {};
     double t_submit = 0.0, t_done = 0.0;
-    bool lean = false;                      // may run in the engine's lean loop
+    int mode = 0;                           // engine loop it needs (0 general, 1 lean, 2 lean+col)
     enum State { kActive, kDone, kFetched } state = kActive;
 };
 
@@ -66,7 +66,8 @@ struct dsmc_server {
     double busy_ms = 0.0;
     unsigned long long last_finished = 0;
     long long stalled = 0;
-    long long general_active = 0;                   // active requests the lean loop cannot run
+    long long general_active = 0;                   // active requests only the general loop runs
+    long long collide_active = 0;                   // active requests needing the collision loop
     char err[512] = {0};
 };
 
@@ -114,9 +115,10 @@ int launch_round(dsmc_server *s) {
     R.lo = s->reqs[static_cast<size_t>(s->active.front())]->inst;
     R.hi = s->engine.serve_instances();
     cudaError_t e = cudaEventRecord(R.start, s->compute);
-    // Rounds run the lean loop while every queued request qualifies for it (same results, fewer
+    // Rounds run the leanest loop every queued request qualifies for (same results, fewer
     // registers and branches); a request published after this launch is not seen by it.
-    if (e == cudaSuccess) e = s->engine.serve_launch(s->compute, s->general_active == 0);
+    const int mode = s->general_active ? 0 : s->collide_active ? 2 : 1;
+    if (e == cudaSuccess) e = s->engine.serve_launch(s->compute, mode);
     if (e == cudaSuccess) s->nlaunches += std::max(1, s->engine.launches_per_graph);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(R.snap, s->engine.serve_counters(), sizeof(dsmc::FastCounters),
@@ -159,7 +161,8 @@ int retire_round(dsmc_server *s) {
         if (done) {
             q.state = Request::kDone;
             q.t_done = t;
-            if (!q.lean) s->general_active--;
+            if (q.mode == 0) s->general_active--;
+            if (q.mode == 2) s->collide_active--;
             s->completed++;
             s->total_steps += static_cast<long long>(q.stats[dsmc::kStatSteps]);
             s->done_queue.push_back(tk);
@@ -338,8 +341,9 @@ int dsmc_server_submit(dsmc_server *s, const dsmc_params *p, const dsmc_surface 
         e = s->engine.serve_append(*p, q->prob->t, n, &q->inst, s->upload, s->compute);
         if (e != cudaSuccess) return cuda_fail(s, "appending to the work queue", e);
         s->active.push_back(tk);
-        q->lean = dsmc::FastEngine::lean_eligible(*p, q->prob->t);
-        if (!q->lean) s->general_active++;
+        q->mode = dsmc::FastEngine::loop_mode(*p, q->prob->t);
+        if (q->mode == 0) s->general_active++;
+        if (q->mode == 2) s->collide_active++;
     } else {
         q->state = Request::kDone;
         q->t_done = q->t_submit;
