@@ -85,6 +85,28 @@ class Stats(C.Structure):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
+class ThermalParams(C.Structure):
+    """ThermalParams (include/thermal.h, the reference's layout)."""
+    _fields_ = [("density", C.c_double), ("conductivity", C.c_double), ("Cp", C.c_double),
+                ("albedo", C.c_double), ("distance_AU", C.c_double), ("depth", C.c_double),
+                ("n_substep", C.c_int), ("z_angle", C.c_double), ("p_mat", C.c_double * 5),
+                ("LH_mat", C.c_double * 5), ("tran_unit_p", C.c_double),
+                ("tran_unit_LH", C.c_double)]
+
+    @staticmethod
+    def default() -> "ThermalParams":
+        tp = ThermalParams()
+        lib().thermal_params_default(C.byref(tp))
+        return tp
+
+
+class SphericalGrid(C.Structure):
+    """SphericalGrid (include/types.h, the reference's layout)."""
+    _fields_ = [("ftd", C.c_int), ("ffd", C.c_int), ("hd", C.c_int),
+                ("density", C.POINTER(C.c_double)), ("temperature", C.POINTER(C.c_double)),
+                ("volume", C.POINTER(C.c_double)), ("horizon", C.POINTER(C.c_double))]
+
+
 class ServerInfo(C.Structure):
     """dsmc_server_info."""
     _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "fetched", "rejected", "active",
@@ -159,6 +181,10 @@ SIGNATURES = [
     ("dsmc_solve_fast_noalloc", C.c_int, [C.POINTER(Params), C.POINTER(Surface), C.c_int64,
                                           C.c_int64, _U64P, _U64P, _U64P, _P]),
     ("dsmc_noalloc_last_error", C.c_char_p, []),
+    ("dsmc_thermal_solve_host", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(ThermalParams), _DP,
+                                          _DP, C.POINTER(C.c_int)]),
+    ("thermal_params_default", None, [C.POINTER(ThermalParams)]),
+    ("thermal_solve", None, [C.POINTER(SphericalGrid), C.POINTER(ThermalParams), _DP, C.c_int]),
     ("dsmc_server_create", C.c_int, [C.c_int, C.c_int64, C.c_int, C.POINTER(_P)]),
     ("dsmc_server_destroy", C.c_int, [_P]),
     ("dsmc_server_last_error", C.c_char_p, [_P]),

@@ -34,6 +34,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CUDA_SOURCES = {
     "kernel_plain.cu": ["-fmad=false"],
     "kernel_fit.cu": ["-fmad=false"],
+    "kernel_thermal.cu": ["-fmad=false"],
     "fast_engine.cu": [],
     "kernel_peak.cu": [],
     "noalloc.cu": [],
@@ -41,7 +42,7 @@ CUDA_SOURCES = {
     "server.cu": [],
     "dsmc_abi.cu": [],
 }
-C_SOURCES = ["host_setup.c", "host_scalar.c", "host_fileio.c", "host_runners.c"]
+C_SOURCES = ["host_setup.c", "host_scalar.c", "host_fileio.c", "host_runners.c", "host_thermal.c"]
 C_FLAGS = ["-O2", "-std=gnu11", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
            "-Wno-unused-parameter", f"-I{INC}", f"-I{CSRC}"]
 

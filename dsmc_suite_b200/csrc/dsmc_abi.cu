@@ -1,6 +1,7 @@
 // dsmc_abi.cu - implementation of the C ABI in include/dsmc_cuda.h: contexts, uploads,
 // launches and result copies. Everything here is host code; the kernels live in kernel_*.cu.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -13,6 +14,7 @@
 #include "problem.h"
 
 extern "C" {
+#include "constants.h"
 #include "types.h"
 #include "velocity.h"
 }
@@ -510,6 +512,95 @@ int dsmc_push_host(dsmc_ctx *c, int path, int64_t n, int nsteps, double *pos, do
     DSMC_CUDA_TRY(c, cudaMemcpyAsync(status, ds, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     if (steps_taken)
         DSMC_CUDA_TRY(c, cudaMemcpyAsync(steps_taken, dt, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_thermal_solve_host(dsmc_ctx *c, int ftd, int ffd, const ThermalParams *tp,
+                            const double *flux, double *T_surface, int *h_depth) {
+    if (!c || !tp || !T_surface || ftd < 1 || ffd < 1 || ftd > 4096 || ffd > 4096)
+        return DSMC_ERR_INVALID;
+    if (tp->n_substep < 1 || !(tp->density > 0.0) || !(tp->conductivity > 0.0) || !(tp->Cp > 0.0) ||
+        !(tp->depth > 0.0) || !(tp->distance_AU > 0.0))
+        return fail(c, DSMC_ERR_INVALID, "thermal parameters must be positive");
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    // scalars of the column model in the reference's operation order (thermal_model.c:110-127)
+    const double P = CONST_P_CERES;
+    const int n_sub = tp->n_substep;
+    const double dt = P / ffd / n_sub;
+    const double kk = tp->conductivity, rho = tp->density, Cp = tp->Cp;
+    const double dr = sqrt(0.1 * 2.0 * dt * kk / rho / Cp);
+    const double hd_real = ceil(tp->depth / dr);
+    if (!(hd_real < 1e6)) return fail(c, DSMC_ERR_INVALID, "thermal column of more than 1e6 points");
+    const int h = hd_real < 3.0 ? 3 : static_cast<int>(hd_real);
+    if (h_depth) *h_depth = h;
+    dsmc::ThermalSetup st{};
+    st.ncol = ftd * ffd;
+    st.h = h;
+    st.n_sub = n_sub;
+    st.R = kk * dt / rho / 2.0 / Cp / (dr * dr);
+    st.k_over_dr = kk / dr;
+    st.a_last = -1.0 / dr;
+    for (int k = 0; k < 5; k++) {
+        st.p[k] = tp->p_mat[k];
+        st.LH[k] = tp->LH_mat[k];
+    }
+    st.tran_p = tp->tran_unit_p;
+    st.tran_LH = tp->tran_unit_LH;
+    st.mmol = CONST_MMOL_H2O;
+    // absorbed flux (the reference's analytic one when none is given, thermal_model.c:130-148),
+    // the initial profile from radiative balance (:172-181), and the coefficients of the
+    // tridiagonal system shared by every column (:230-244, forward sweep of :80-103)
+    const size_t ncol = static_cast<size_t>(st.ncol);
+    std::vector<double> F(ncol), qT0(ncol * h), cpv(h), piv(h);
+    const double Si = CONST_SOLAR_1AU * (1.0 / tp->distance_AU) * (1.0 / tp->distance_AU);
+    const double dF = Si * (1.0 - tp->albedo);
+    for (int td = 0; td < ftd; td++)
+        for (int fd = 0; fd < ffd; fd++) {
+            double f;
+            if (flux) {
+                f = flux[td * ffd + fd];
+            } else {
+                const double thi = (td + 0.5) / ftd * M_PI - M_PI / 2.0;
+                const double fi = (fd + 0.5) / ffd * 2.0 * M_PI;
+                f = fi >= M_PI ? 0.0 : dF * cos(thi) * sin(fi);
+            }
+            F[td * ffd + fd] = fabs(f);
+        }
+    for (size_t k = 0; k < ncol; k++) {
+        const double T_init = F[k] > 0 ? pow(F[k] / CONST_SIGMA, 0.25) : 100.0;
+        for (int d = 0; d < h; d++) qT0[static_cast<size_t>(d) * ncol + k] = T_init;
+    }
+    cpv[0] = 0.0 / 1.0;
+    piv[0] = 1.0;
+    for (int i = 1; i < h; i++) {
+        const double ai = i < h - 1 ? -st.R : st.a_last;
+        const double bi = i < h - 1 ? 1.0 + 2.0 * st.R : 1.0 / dr;
+        const double ci = i < h - 1 ? -st.R : 0.0;
+        piv[i] = bi - ai * cpv[i - 1];
+        cpv[i] = ci / piv[i];
+    }
+    struct Bufs {
+        void *p[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        ~Bufs() { for (void *q : p) if (q) cudaFree(q); }
+    } b;
+    const size_t prof = ncol * h * sizeof(double);
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[0], ncol * sizeof(double)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[1], h * sizeof(double)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[2], h * sizeof(double)));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[3], prof));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[4], prof));
+    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[5], ncol * sizeof(double)));
+    double *dF_ = static_cast<double *>(b.p[0]), *dcp = static_cast<double *>(b.p[1]);
+    double *dpiv = static_cast<double *>(b.p[2]), *dq = static_cast<double *>(b.p[3]);
+    double *ddp = static_cast<double *>(b.p[4]), *dT = static_cast<double *>(b.p[5]);
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(dF_, F.data(), ncol * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(dcp, cpv.data(), h * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(dpiv, piv.data(), h * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(dq, qT0.data(), prof, cudaMemcpyHostToDevice, c->stream));
+    DSMC_CUDA_TRY(c, dsmc::launch_thermal(st, dF_, dcp, dpiv, dq, ddp, dT, c->stream));
+    DSMC_CUDA_TRY(c, cudaMemcpyAsync(T_surface, dT, ncol * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return DSMC_OK;
 }

@@ -32,4 +32,17 @@ cudaError_t launch_fit_hist(int ncell, int nbins, double bin_width, const unsign
                             int degree, double *coef, double *box, double *total, int *valid,
                             cudaStream_t stream);
 
+// Thermal column model (kernel_thermal.cu): scalars of one solve, formed on the host in the
+// reference's operation order.
+struct ThermalSetup {
+    int ncol, h, n_sub;
+    double R, k_over_dr, a_last;
+    double p[5], LH[5], tran_p, tran_LH, mmol;
+};
+// flux [ncol] = |F|; cp, piv [h]; qT [h][ncol] holds the initial profiles and receives the final
+// ones; dp [h][ncol] scratch; T_surface [ncol].
+cudaError_t launch_thermal(const ThermalSetup &s, const double *flux, const double *cp,
+                           const double *piv, double *qT, double *dp, double *T_surface,
+                           cudaStream_t stream);
+
 }  // namespace dsmc

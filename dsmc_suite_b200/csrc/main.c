@@ -1,13 +1,38 @@
 /* main.c - the dsmc_suite command line (flags and subcommands of the reference's
- * src/main.c:52-213). dsmc and dsmc-adv run on the GPU through the drop-in runners; pipeline
- * chains them through the same files as the reference (main.c:153-205). The thermal model and
- * the Embree ray tracer are not part of this build: thermal and raytrace report that and exit 1,
- * and pipeline needs an existing temperature file (-T). */
+ * src/main.c:52-213). dsmc, dsmc-adv and thermal run on the GPU through the drop-in runners and
+ * thermal_solve; pipeline chains thermal -> dsmc -> dsmc-adv through the same files as the
+ * reference (main.c:153-205). The Embree ray tracer is not part of this build: raytrace reports
+ * that and exits 1, and pipeline skips its ray-tracing step as the reference does without a mesh. */
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include "dsmc_runners.h"
+#include "grid.h"
+#include "thermal.h"
+
+/* thermal model on the 36 x 72 grid, written as <prefix>_temperature.dat (main.c:118-143) */
+static int run_thermal(const char *output_prefix, const double *za_deg, int nthreads, char *t_file,
+                       size_t t_len)
+{
+    const int ftd = 36, ffd = 72;
+    SphericalGrid *grid = grid_create(ftd, ffd, 1);
+    if (!grid) { fprintf(stderr, "out of host memory\n"); return 1; }
+    ThermalParams tp;
+    thermal_params_default(&tp);
+    if (za_deg) tp.z_angle = *za_deg / 180.0 * M_PI;
+    thermal_solve(grid, &tp, NULL, nthreads);
+    if (isnan(grid->temperature[0])) { grid_free(grid); return 1; }   /* the solve failed */
+    snprintf(t_file, t_len, "%s_temperature.dat", output_prefix);
+    FILE *fp = fopen(t_file, "w");
+    if (!fp) { fprintf(stderr, "cannot write %s\n", t_file); grid_free(grid); return 1; }
+    fprintf(fp, "%d\n%d\n", ftd, ffd);
+    for (int k = 0; k < ftd * ffd; k++) fprintf(fp, "%8.6f\n", grid->temperature[k]);
+    fclose(fp);
+    grid_free(grid);
+    return 0;
+}
 
 static void print_usage(const char *prog)
 {
@@ -16,7 +41,8 @@ static void print_usage(const char *prog)
     printf("Commands:\n");
     printf("  dsmc      - Basic ballistic DSMC (no collisions)\n");
     printf("  dsmc-adv  - Advanced DSMC with collisions\n");
-    printf("  pipeline  - dsmc then dsmc-adv on the same temperature file\n\n");
+    printf("  thermal   - 1D spherical thermal diffusion model (GPU)\n");
+    printf("  pipeline  - thermal, then dsmc, then dsmc-adv\n\n");
     printf("Options:\n");
     printf("  -n <particles>     Number of test particles (default: 10000)\n");
     printf("  -t <threads>       Accepted for compatibility (the solve runs on one GPU)\n");
@@ -34,6 +60,7 @@ int main(int argc, char *argv[])
     int totaln = 10000, nthreads = 1;
     const char *temp_file = "Ceres_T_VP.dat", *den_file = NULL, *v_record_file = NULL;
     const char *output_prefix = "output";
+    double za_deg = 12.3;
     for (int i = 2; i < argc; i++) {
         const int more = i + 1 < argc;
         if (!strcmp(argv[i], "-n") && more) totaln = atoi(argv[++i]);
@@ -42,28 +69,36 @@ int main(int argc, char *argv[])
         else if (!strcmp(argv[i], "-d") && more) den_file = argv[++i];
         else if (!strcmp(argv[i], "-v") && more) v_record_file = argv[++i];
         else if (!strcmp(argv[i], "-o") && more) output_prefix = argv[++i];
+        else if (!strcmp(argv[i], "--za") && more) za_deg = atof(argv[++i]);
         else if ((!strcmp(argv[i], "-m") || !strcmp(argv[i], "-f") || !strcmp(argv[i], "--npoint") ||
-                  !strcmp(argv[i], "--nface") || !strcmp(argv[i], "--za") ||
-                  !strcmp(argv[i], "--tt") || !strcmp(argv[i], "--nmonte")) && more)
-            ++i;   /* ray-tracer and thermal flags: accepted and ignored */
+                  !strcmp(argv[i], "--nface") || !strcmp(argv[i], "--tt") ||
+                  !strcmp(argv[i], "--nmonte")) && more)
+            ++i;   /* ray-tracer flags: accepted and ignored */
     }
     if (!strcmp(command, "dsmc")) {
         run_ballistic(totaln, temp_file, output_prefix, nthreads);
     } else if (!strcmp(command, "dsmc-adv")) {
         run_advanced(totaln, temp_file, den_file, v_record_file, output_prefix, nthreads);
+    } else if (!strcmp(command, "thermal")) {
+        char t_file[1100];
+        if (run_thermal(output_prefix, &za_deg, nthreads, t_file, sizeof t_file)) return 1;
     } else if (!strcmp(command, "pipeline")) {
-        char p1[1024], p2[1024], den[1100], vr[1100];
+        char t_file[1100], p1[1024], p2[1024], den[1100], vr[1100];
+        printf("=== FULL PIPELINE ===\n\n");
+        printf("--- Step 1: Skipped (no ray tracer in this build) ---\n");
+        printf("\n--- Step 2: Thermal Model ---\n");
+        if (run_thermal(output_prefix, NULL, nthreads, t_file, sizeof t_file)) return 1;
         snprintf(p1, sizeof p1, "%s_phase1", output_prefix);
         snprintf(p2, sizeof p2, "%s_phase2", output_prefix);
         snprintf(den, sizeof den, "%s_den.dat", p1);
         snprintf(vr, sizeof vr, "%s_v_record.dat", p1);
-        printf("=== PIPELINE (phases 3-4) ===\n\n--- Basic DSMC ---\n");
-        run_ballistic(totaln, temp_file, p1, nthreads);
-        printf("\n--- Advanced DSMC ---\n");
-        run_advanced(totaln, temp_file, den, vr, p2, nthreads);
+        printf("\n--- Step 3: Basic DSMC ---\n");
+        run_ballistic(totaln, t_file, p1, nthreads);
+        printf("\n--- Step 4: Advanced DSMC ---\n");
+        run_advanced(totaln, t_file, den, vr, p2, nthreads);
         printf("\n=== PIPELINE COMPLETE ===\n");
-    } else if (!strcmp(command, "thermal") || !strcmp(command, "raytrace")) {
-        fprintf(stderr, "%s: not part of this build (the DSMC hot path only)\n", command);
+    } else if (!strcmp(command, "raytrace")) {
+        fprintf(stderr, "%s: not part of this build (no ray tracer)\n", command);
         return 1;
     } else {
         fprintf(stderr, "Unknown command: %s\n", command);

@@ -175,6 +175,19 @@ class Context:
         k = nrec.value
         return v[:k], td[:k], fd[:k], ht[:k]
 
+    # thermal model -----------------------------------------------------------------------------
+    def thermal(self, ftd: int = 36, ffd: int = 72, tp: N.ThermalParams | None = None,
+                flux: np.ndarray | None = None) -> tuple[np.ndarray, int]:
+        """Surface temperature [ftd][ffd] of the thermal column model on the device, and the
+        number of depth points."""
+        tp = N.ThermalParams.default() if tp is None else tp
+        F = None if flux is None else np.ascontiguousarray(flux, dtype=np.float64)
+        T = np.zeros((ftd, ffd))
+        h = C.c_int()
+        self._check(self._lib.dsmc_thermal_solve_host(self.h, ftd, ffd, C.byref(tp), N.ptr(F),
+                                                      N.ptr(T), C.byref(h)), "thermal")
+        return T, h.value
+
     # one-call solve ---------------------------------------------------------------------------
     def solve(self, path: int, params: N.Params, surface: N.SurfaceInputs, n: int,
               collision: N.CollisionInputs | None = None, outputs: bool = False) -> dict:

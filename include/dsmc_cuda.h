@@ -21,6 +21,7 @@
 #include <stddef.h>
 #include <stdint.h>
 #include "dsmc_params.h"
+#include "thermal.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -222,6 +223,16 @@ int dsmc_solve_fast_noalloc(const dsmc_params *p, const dsmc_surface *surf, int6
                             int64_t n, uint64_t *density, uint64_t *horizon, uint64_t *stats,
                             void *stream);
 const char *dsmc_noalloc_last_error(void);
+
+/* ---- Thermal model -------------------------------------------------------------------------- */
+/* Replaces the column loop of thermal_solve (src/thermal/thermal_model.c:105-283): the 1-D heat  */
+/* equation of every surface cell, n_substep implicit steps of one rotation step each, with the  */
+/* surface temperature from the energy balance (solar flux, conduction, thermal emission, H2O    */
+/* sublimation) by bisection and a zero-flux bottom. One GPU thread per (td, fd) column, FP64.   */
+/* flux [ftd][ffd] absorbed flux [W/m^2], or NULL for the reference's analytic flux; writes the  */
+/* surface temperature T_surface [ftd][ffd] and, when h_depth is not NULL, the depth points.     */
+int dsmc_thermal_solve_host(dsmc_ctx *ctx, int ftd, int ffd, const ThermalParams *tp,
+                            const double *flux, double *T_surface, int *h_depth);
 
 /* ---- Batched and served solves ------------------------------------------------------------- */
 /* No counterpart in the reference, whose runners solve one problem per call                   */

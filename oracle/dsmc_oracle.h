@@ -17,6 +17,7 @@
 
 #include <stdint.h>
 #include "../include/dsmc_params.h"
+#include "../include/thermal.h"
 
 enum { OR_RNG_RAND_R = 0, OR_RNG_PHILOX = 1 };
 
@@ -73,5 +74,10 @@ int or_locate_face(const dsmc_surface *surf, const double p[3]);
 int or_run(const dsmc_params *p, const dsmc_surface *surf, const dsmc_collision *col,
            const or_vtable *vt, int rng_kind, unsigned rr_seed, int64_t pid_begin, int64_t n,
            int nthreads, or_outputs *out);
+
+/* Thermal column model (thermal_oracle.c): surface temperature [ftd][ffd]; flux NULL = the
+ * reference's analytic flux. Returns 0, or < 0 on bad input / no memory. */
+int or_thermal_solve(int ftd, int ffd, const ThermalParams *tp, const double *flux,
+                     double *T_out, int *h_depth);
 
 #endif

@@ -76,6 +76,9 @@ def lib() -> C.CDLL:
         L.or_velocity_sample_word.argtypes = [C.POINTER(VTable), C.c_double, C.c_uint32]
         L.or_cdf_sample.restype = C.c_double
         L.or_cdf_sample.argtypes = [D, D, C.c_double, C.c_int, C.c_double]
+        L.or_thermal_solve.restype = C.c_int
+        L.or_thermal_solve.argtypes = [C.c_int, C.c_int, C.POINTER(N.ThermalParams), D, D,
+                                       C.POINTER(C.c_int)]
         L.or_polyfit.restype = C.c_int
         L.or_polyfit.argtypes = [D, D, C.c_int, C.c_int, D]
         L.or_fit_cell_from_samples.restype = C.c_int
@@ -161,3 +164,33 @@ def run(params, surface, n: int, collision=None, rng: int = RNG_PHILOX, rr_seed:
             res[name] = res[name][:k]
     del nh
     return res
+
+
+def thermal(ftd: int, ffd: int, tp, flux: np.ndarray | None = None) -> tuple[np.ndarray, int]:
+    """The oracle's thermal column model: surface temperature [ftd][ffd] and depth points."""
+    F = None if flux is None else np.ascontiguousarray(flux, dtype=np.float64)
+    T = np.zeros((ftd, ffd))
+    h = C.c_int()
+    rc = lib().or_thermal_solve(ftd, ffd, C.byref(tp), _p(F) if F is not None else None, _p(T),
+                                C.byref(h))
+    if rc != 0:
+        raise RuntimeError(f"or_thermal_solve failed: {rc}")
+    return T, h.value
+
+
+def reference_thermal(ftd: int, ffd: int, tp, flux: np.ndarray | None = None) -> np.ndarray | None:
+    """The reference's own thermal_solve (oracle/_ref/libdsmcref.so), or None when that build is
+    absent. Its stdout lines go to the process's stdout."""
+    so = REF_DIR / "libdsmcref.so"
+    if not so.exists():
+        return None
+    from dsmc_suite_b200 import _native as N
+    R = C.CDLL(str(so))
+    R.thermal_solve.restype = None
+    R.thermal_solve.argtypes = [C.POINTER(N.SphericalGrid), C.POINTER(N.ThermalParams),
+                                C.POINTER(C.c_double), C.c_int]
+    T = np.zeros((ftd, ffd))
+    g = N.SphericalGrid(ftd=ftd, ffd=ffd, hd=1, temperature=_p(T))
+    F = None if flux is None else np.ascontiguousarray(flux, dtype=np.float64)
+    R.thermal_solve(C.byref(g), C.byref(tp), _p(F) if F is not None else None, 1)
+    return T

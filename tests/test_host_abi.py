@@ -224,7 +224,7 @@ def test_cli_usage_and_out_of_scope_commands(built):
     cli = ROOT / "dsmc_suite_b200" / "bin" / "dsmc_suite"
     r = subprocess.run([str(cli)], capture_output=True, text=True)
     assert r.returncode == 1 and "dsmc-adv" in r.stdout
-    r = subprocess.run([str(cli), "thermal"], capture_output=True, text=True)
+    r = subprocess.run([str(cli), "raytrace"], capture_output=True, text=True)
     assert r.returncode == 1 and "not part of this build" in r.stderr
     r = subprocess.run([str(cli), "bogus"], capture_output=True, text=True)
     assert r.returncode == 1 and "Unknown command" in r.stderr

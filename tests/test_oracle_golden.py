@@ -13,7 +13,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from conftest import ROOT, cold_T
+from conftest import GOLDEN, ROOT, cold_T
 
 
 def test_philox_known_answers(O):
@@ -234,3 +234,23 @@ def test_live_reference_ballistic_small(N, O, tmp_path, n):
     den = f"36\n72\n{p.hd}\n" + _fmt(r["density_f64"].ravel(), "%9.6f")
     assert den == (tmp_path / "r_den.dat").read_text()
     assert _fmt(r["ttime"][:5].ravel(), "%9.5f") == (tmp_path / "r_ttime.dat").read_text()
+
+
+def _thermal_cases(N):
+    import sys
+    sys.path.insert(0, str(GOLDEN))
+    import make_thermal_golden as G
+    return G.cases(N)
+
+
+def test_thermal_oracle_matches_reference(N, O):
+    """The oracle's thermal column model equals the reference's thermal_solve bit for bit: against
+    the committed fixture (made by the reference build), and live where oracle/_ref exists."""
+    g = np.load(GOLDEN / "reference_thermal.npz")
+    for name, ftd, ffd, tp, flux in _thermal_cases(N):
+        T, h = O.thermal(ftd, ffd, tp, flux)
+        np.testing.assert_array_equal(T, g[name])
+        assert h >= 3
+        live = O.reference_thermal(ftd, ffd, tp, flux)
+        if live is not None:
+            np.testing.assert_array_equal(T, live)
