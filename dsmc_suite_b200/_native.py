@@ -107,6 +107,33 @@ class SphericalGrid(C.Structure):
                 ("volume", C.POINTER(C.c_double)), ("horizon", C.POINTER(C.c_double))]
 
 
+class Vec3(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+
+class Mesh(C.Structure):
+    """Mesh (include/types.h, the reference's layout)."""
+    _fields_ = [("npoint", C.c_int), ("nface", C.c_int), ("spot", C.POINTER(C.c_double)),
+                ("facet", C.POINTER(C.c_int)), ("face_normal", C.POINTER(C.c_double)),
+                ("face_area", C.POINTER(C.c_double)), ("loc_xyz", C.POINTER(C.c_double)),
+                ("dir", C.POINTER(C.c_double))]
+
+
+def mesh_normals(spot: np.ndarray, facet: np.ndarray) -> dict:
+    """The kept mesh_compute_normals on numpy arrays: spot [npoint][3], facet [nface][3] 0-based.
+    Returns normals, areas, centroids and (latitude, longitude) directions."""
+    spot = np.ascontiguousarray(spot, dtype=np.float64)
+    facet = np.ascontiguousarray(facet, dtype=np.int32)
+    nf = facet.shape[0]
+    out = {"normal": np.zeros((nf, 3)), "area": np.zeros(nf), "centroid": np.zeros((nf, 3)),
+           "dir": np.zeros((nf, 2))}
+    m = Mesh(npoint=spot.shape[0], nface=nf, spot=ptr(spot), facet=ptr(facet, C.c_int),
+             face_normal=ptr(out["normal"]), face_area=ptr(out["area"]),
+             loc_xyz=ptr(out["centroid"]), dir=ptr(out["dir"]))
+    lib().mesh_compute_normals(C.byref(m))
+    return out
+
+
 class ServerInfo(C.Structure):
     """dsmc_server_info."""
     _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "fetched", "rejected", "active",
@@ -185,6 +212,14 @@ SIGNATURES = [
                                           _DP, C.POINTER(C.c_int)]),
     ("thermal_params_default", None, [C.POINTER(ThermalParams)]),
     ("thermal_solve", None, [C.POINTER(SphericalGrid), C.POINTER(ThermalParams), _DP, C.c_int]),
+    ("dsmc_shadow_flux_host", C.c_int, [_P, C.c_int, _DP, C.c_int, _I32P, _DP, C.c_double,
+                                        C.c_int, C.c_int, _DP]),
+    ("mesh_load", C.POINTER(Mesh), [C.c_char_p, C.c_char_p, C.c_int, C.c_int]),
+    ("mesh_free", None, [C.POINTER(Mesh)]),
+    ("mesh_compute_normals", None, [C.POINTER(Mesh)]),
+    ("random_point_on_triangle", Vec3, [Vec3, Vec3, Vec3, C.POINTER(C.c_uint)]),
+    ("run_raytracer", None, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int,
+                             C.c_int, C.c_char_p, C.c_int]),
     ("dsmc_server_create", C.c_int, [C.c_int, C.c_int64, C.c_int, C.POINTER(_P)]),
     ("dsmc_server_destroy", C.c_int, [_P]),
     ("dsmc_server_last_error", C.c_char_p, [_P]),

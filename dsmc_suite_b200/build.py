@@ -35,6 +35,7 @@ CUDA_SOURCES = {
     "kernel_plain.cu": ["-fmad=false"],
     "kernel_fit.cu": ["-fmad=false"],
     "kernel_thermal.cu": ["-fmad=false"],
+    "kernel_raytrace.cu": ["-fmad=false"],
     "fast_engine.cu": [],
     "kernel_peak.cu": [],
     "noalloc.cu": [],
@@ -42,7 +43,8 @@ CUDA_SOURCES = {
     "server.cu": [],
     "dsmc_abi.cu": [],
 }
-C_SOURCES = ["host_setup.c", "host_scalar.c", "host_fileio.c", "host_runners.c", "host_thermal.c"]
+C_SOURCES = ["host_setup.c", "host_scalar.c", "host_fileio.c", "host_runners.c", "host_thermal.c",
+             "host_raytrace.c"]
 C_FLAGS = ["-O2", "-std=gnu11", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
            "-Wno-unused-parameter", f"-I{INC}", f"-I{CSRC}"]
 

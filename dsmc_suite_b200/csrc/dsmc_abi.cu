@@ -605,6 +605,24 @@ int dsmc_thermal_solve_host(dsmc_ctx *c, int ftd, int ffd, const ThermalParams *
     return DSMC_OK;
 }
 
+int dsmc_shadow_flux_host(dsmc_ctx *c, int npoint, const double *spot, int nface,
+                          const int32_t *facet, const double *face_normal, double za, int tt,
+                          int nmonte, double *F) {
+    if (!c || !spot || !facet || !face_normal || !F || npoint < 3 || nface < 1 || tt < 1 ||
+        nmonte < 1 || static_cast<long long>(nface) * tt > (1ll << 31))
+        return DSMC_ERR_INVALID;
+    for (long long k = 0; k < 3ll * nface; k++)
+        if (facet[k] < 0 || facet[k] >= npoint)
+            return fail(c, DSMC_ERR_INVALID, "face %lld names vertex %d of %d", k / 3, facet[k], npoint);
+    int rc = set_device(c);
+    if (rc != DSMC_OK) return rc;
+    long long overflows = 0;
+    DSMC_CUDA_TRY(c, dsmc::shadow_flux(npoint, spot, nface, facet, face_normal, za, tt, nmonte, F,
+                                       c->stream, &overflows));
+    if (overflows) return fail(c, DSMC_ERR_INVALID, "BVH deeper than the traversal stack");
+    return DSMC_OK;
+}
+
 int dsmc_velocity_record(dsmc_ctx *c, int64_t n, int per_bucket, int64_t total_cap,
                          double *v_out, int32_t *td, int32_t *fd, int32_t *ht, int64_t *n_out) {
     if (!c || !v_out || !td || !fd || !ht || !n_out || n < 0 || per_bucket < 1 || total_cap < 0)

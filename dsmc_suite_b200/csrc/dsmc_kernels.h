@@ -45,4 +45,11 @@ cudaError_t launch_thermal(const ThermalSetup &s, const double *flux, const doub
                            const double *piv, double *qT, double *dp, double *T_surface,
                            cudaStream_t stream);
 
+// Monte Carlo shadow flux (kernel_raytrace.cu): builds the BVH of the mesh on the host, traces
+// on `stream` and copies F [nface][tt] back (synchronous). *overflows counts traversal-stack
+// overflows (0 for meshes below 2^24 faces).
+cudaError_t shadow_flux(int npoint, const double *spot, int nface, const int *facet,
+                        const double *normal, double za, int tt, int nmonte, double *F_host,
+                        cudaStream_t stream, long long *overflows);
+
 }  // namespace dsmc

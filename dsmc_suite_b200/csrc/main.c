@@ -1,8 +1,8 @@
 /* main.c - the dsmc_suite command line (flags and subcommands of the reference's
  * src/main.c:52-213). dsmc, dsmc-adv and thermal run on the GPU through the drop-in runners and
- * thermal_solve; pipeline chains thermal -> dsmc -> dsmc-adv through the same files as the
- * reference (main.c:153-205). The Embree ray tracer is not part of this build: raytrace reports
- * that and exits 1, and pipeline skips its ray-tracing step as the reference does without a mesh. */
+ * thermal_solve, raytrace through run_raytracer (shadow rays on the GPU instead of Embree);
+ * pipeline chains raytrace (when a mesh is given) -> thermal -> dsmc -> dsmc-adv through the same
+ * files as the reference (main.c:153-205). */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -10,6 +10,7 @@
 
 #include "dsmc_runners.h"
 #include "grid.h"
+#include "raytracer.h"
 #include "thermal.h"
 
 /* thermal model on the 36 x 72 grid, written as <prefix>_temperature.dat (main.c:118-143) */
@@ -41,6 +42,7 @@ static void print_usage(const char *prog)
     printf("Commands:\n");
     printf("  dsmc      - Basic ballistic DSMC (no collisions)\n");
     printf("  dsmc-adv  - Advanced DSMC with collisions\n");
+    printf("  raytrace  - MC shadow flux of a mesh (GPU BVH)\n");
     printf("  thermal   - 1D spherical thermal diffusion model (GPU)\n");
     printf("  pipeline  - thermal, then dsmc, then dsmc-adv\n\n");
     printf("Options:\n");
@@ -61,6 +63,8 @@ int main(int argc, char *argv[])
     const char *temp_file = "Ceres_T_VP.dat", *den_file = NULL, *v_record_file = NULL;
     const char *output_prefix = "output";
     double za_deg = 12.3;
+    const char *vertex_file = NULL, *face_file = NULL;
+    int npoint = 0, nface_mesh = 0, tt = 24, nmonte = 50;
     for (int i = 2; i < argc; i++) {
         const int more = i + 1 < argc;
         if (!strcmp(argv[i], "-n") && more) totaln = atoi(argv[++i]);
@@ -70,10 +74,12 @@ int main(int argc, char *argv[])
         else if (!strcmp(argv[i], "-v") && more) v_record_file = argv[++i];
         else if (!strcmp(argv[i], "-o") && more) output_prefix = argv[++i];
         else if (!strcmp(argv[i], "--za") && more) za_deg = atof(argv[++i]);
-        else if ((!strcmp(argv[i], "-m") || !strcmp(argv[i], "-f") || !strcmp(argv[i], "--npoint") ||
-                  !strcmp(argv[i], "--nface") || !strcmp(argv[i], "--tt") ||
-                  !strcmp(argv[i], "--nmonte")) && more)
-            ++i;   /* ray-tracer flags: accepted and ignored */
+        else if (!strcmp(argv[i], "-m") && more) vertex_file = argv[++i];
+        else if (!strcmp(argv[i], "-f") && more) face_file = argv[++i];
+        else if (!strcmp(argv[i], "--npoint") && more) npoint = atoi(argv[++i]);
+        else if (!strcmp(argv[i], "--nface") && more) nface_mesh = atoi(argv[++i]);
+        else if (!strcmp(argv[i], "--tt") && more) tt = atoi(argv[++i]);
+        else if (!strcmp(argv[i], "--nmonte") && more) nmonte = atoi(argv[++i]);
     }
     if (!strcmp(command, "dsmc")) {
         run_ballistic(totaln, temp_file, output_prefix, nthreads);
@@ -85,7 +91,15 @@ int main(int argc, char *argv[])
     } else if (!strcmp(command, "pipeline")) {
         char t_file[1100], p1[1024], p2[1024], den[1100], vr[1100];
         printf("=== FULL PIPELINE ===\n\n");
-        printf("--- Step 1: Skipped (no ray tracer in this build) ---\n");
+        if (vertex_file && face_file && npoint > 0 && nface_mesh > 0) {
+            char flux_file[1100];
+            snprintf(flux_file, sizeof flux_file, "%s_flux.dat", output_prefix);
+            printf("--- Step 1: Ray Tracing ---\n");
+            run_raytracer(vertex_file, face_file, npoint, nface_mesh, za_deg, tt, nmonte, flux_file,
+                          nthreads);
+        } else {
+            printf("--- Step 1: Skipped (no mesh provided) ---\n");
+        }
         printf("\n--- Step 2: Thermal Model ---\n");
         if (run_thermal(output_prefix, NULL, nthreads, t_file, sizeof t_file)) return 1;
         snprintf(p1, sizeof p1, "%s_phase1", output_prefix);
@@ -98,8 +112,14 @@ int main(int argc, char *argv[])
         run_advanced(totaln, t_file, den, vr, p2, nthreads);
         printf("\n=== PIPELINE COMPLETE ===\n");
     } else if (!strcmp(command, "raytrace")) {
-        fprintf(stderr, "%s: not part of this build (no ray tracer)\n", command);
-        return 1;
+        if (!vertex_file || !face_file || npoint <= 0 || nface_mesh <= 0) {
+            fprintf(stderr, "raytrace requires -m <vertex_file> -f <face_file> --npoint <n> --nface <n>\n");
+            return 1;
+        }
+        char flux_file[1100];
+        snprintf(flux_file, sizeof flux_file, "%s_flux.dat", output_prefix);
+        run_raytracer(vertex_file, face_file, npoint, nface_mesh, za_deg, tt, nmonte, flux_file,
+                      nthreads);
     } else {
         fprintf(stderr, "Unknown command: %s\n", command);
         print_usage(argv[0]);

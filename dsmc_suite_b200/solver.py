@@ -188,6 +188,20 @@ class Context:
                                                       N.ptr(T), C.byref(h)), "thermal")
         return T, h.value
 
+    # shadow flux ------------------------------------------------------------------------------
+    def shadow_flux(self, spot: np.ndarray, facet: np.ndarray, normal: np.ndarray, za: float,
+                    tt: int = 24, nmonte: int = 50) -> np.ndarray:
+        """F [nface][tt] of the Monte Carlo shadow model on the device (za in radians)."""
+        spot = np.ascontiguousarray(spot, dtype=np.float64)
+        facet = np.ascontiguousarray(facet, dtype=np.int32)
+        normal = np.ascontiguousarray(normal, dtype=np.float64)
+        F = np.zeros((facet.shape[0], tt))
+        self._check(self._lib.dsmc_shadow_flux_host(self.h, spot.shape[0], N.ptr(spot),
+                                                    facet.shape[0], N.ptr(facet, C.c_int32),
+                                                    N.ptr(normal), za, tt, nmonte, N.ptr(F)),
+                    "shadow_flux")
+        return F
+
     # one-call solve ---------------------------------------------------------------------------
     def solve(self, path: int, params: N.Params, surface: N.SurfaceInputs, n: int,
               collision: N.CollisionInputs | None = None, outputs: bool = False) -> dict:

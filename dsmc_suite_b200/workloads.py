@@ -229,3 +229,26 @@ def served_stream(ctx, rate_hz: float, seconds: float, seed: int = 20261203,
         out.append((t, req))
         k += 1
     return out
+
+
+# ------------------------------------------------------------------------------------------
+# Synthetic body mesh for the shadow-flux model (no mesh files ship with the reference)
+
+
+def cratered_mesh(nlevel: int = 4, craters: int = 16, depth: float = 0.15, width: float = 0.25,
+                  seed: int = 20261203, radius: float = 1.0):
+    """Icosphere of 20 * 4^nlevel faces with Gaussian craters pressed into it (concave, so faces
+    shadow each other at low sun). Returns (spot [npoint][3], facet [nface][3] 0-based)."""
+    ico = N.Icosphere(nlevel)
+    fv = ico.face_verts.reshape(-1, 3)
+    key = np.round(fv, 12)
+    uniq, inv = np.unique(key, axis=0, return_inverse=True)
+    spot = uniq.astype(np.float64)
+    facet = inv.reshape(-1, 3).astype(np.int32)
+    rng = np.random.default_rng(seed)
+    c = rng.normal(size=(craters, 3))
+    c /= np.linalg.norm(c, axis=1, keepdims=True)
+    u = spot / np.linalg.norm(spot, axis=1, keepdims=True)
+    d2 = ((u[:, None, :] - c[None, :, :]) ** 2).sum(-1)
+    r = radius * (1.0 - depth * np.exp(-d2 / (width * width)).sum(1).clip(max=1.0))
+    return u * r[:, None], facet

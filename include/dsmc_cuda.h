@@ -234,6 +234,17 @@ const char *dsmc_noalloc_last_error(void);
 int dsmc_thermal_solve_host(dsmc_ctx *ctx, int ftd, int ffd, const ThermalParams *tp,
                             const double *flux, double *T_surface, int *h_depth);
 
+/* ---- Shadow flux ------------------------------------------------------------------------------ */
+/* Replaces the Embree loop of the reference's ray tracer (src/raytracer/shadow_maker.c:198-238):  */
+/* for rotation phase t in [0, tt) and face f, F[f][t] = (1 - shadowed / nmonte) (s . n_f), 0 when  */
+/* s . n_f < 0, with s the sun direction at declination -za [rad] and the shadow rays from nmonte  */
+/* rand_r points of the face (seed t * nface + f + 42) lifted 1e-3 along n_f. spot [npoint][3]     */
+/* vertices, facet [nface][3] 0-based vertex indices, face_normal [nface][3] outward unit normals   */
+/* (mesh_compute_normals). The mesh's BVH is built on the host; the rays are traced on the GPU.   */
+int dsmc_shadow_flux_host(dsmc_ctx *ctx, int npoint, const double *spot, int nface,
+                          const int32_t *facet, const double *face_normal, double za, int tt,
+                          int nmonte, double *F);
+
 /* ---- Batched and served solves ------------------------------------------------------------- */
 /* No counterpart in the reference, whose runners solve one problem per call                   */
 /* (src/dsmc/ballistic.c:38, src/dsmc/advanced.c:132). A server owns one GPU: a fixed set of     */

@@ -80,4 +80,8 @@ int or_run(const dsmc_params *p, const dsmc_surface *surf, const dsmc_collision 
 int or_thermal_solve(int ftd, int ffd, const ThermalParams *tp, const double *flux,
                      double *T_out, int *h_depth);
 
+/* Monte Carlo shadow flux (raytrace_oracle.c): F [nface][tt]; facet 0-based. */
+int or_shadow_flux(int npoint, const double *spot, int nface, const int32_t *facet,
+                   const double *normal, double za, int tt, int nmonte, double *F, int nthreads);
+
 #endif

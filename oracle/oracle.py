@@ -79,6 +79,9 @@ def lib() -> C.CDLL:
         L.or_thermal_solve.restype = C.c_int
         L.or_thermal_solve.argtypes = [C.c_int, C.c_int, C.POINTER(N.ThermalParams), D, D,
                                        C.POINTER(C.c_int)]
+        L.or_shadow_flux.restype = C.c_int
+        L.or_shadow_flux.argtypes = [C.c_int, D, C.c_int, C.POINTER(C.c_int32), D, C.c_double,
+                                     C.c_int, C.c_int, D, C.c_int]
         L.or_polyfit.restype = C.c_int
         L.or_polyfit.argtypes = [D, D, C.c_int, C.c_int, D]
         L.or_fit_cell_from_samples.restype = C.c_int
@@ -194,3 +197,16 @@ def reference_thermal(ftd: int, ffd: int, tp, flux: np.ndarray | None = None) ->
     F = None if flux is None else np.ascontiguousarray(flux, dtype=np.float64)
     R.thermal_solve(C.byref(g), C.byref(tp), _p(F) if F is not None else None, 1)
     return T
+
+
+def shadow_flux(spot, facet, normal, za: float, tt: int, nmonte: int, nthreads: int = 8):
+    """The oracle's Monte Carlo shadow flux F [nface][tt] (brute-force occlusion)."""
+    spot = np.ascontiguousarray(spot, dtype=np.float64)
+    facet = np.ascontiguousarray(facet, dtype=np.int32)
+    normal = np.ascontiguousarray(normal, dtype=np.float64)
+    F = np.zeros((facet.shape[0], tt))
+    rc = lib().or_shadow_flux(spot.shape[0], _p(spot), facet.shape[0], _p(facet, C.c_int32),
+                              _p(normal), za, tt, nmonte, _p(F), nthreads)
+    if rc != 0:
+        raise RuntimeError(f"or_shadow_flux failed: {rc}")
+    return F

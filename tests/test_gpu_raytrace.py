@@ -1,0 +1,81 @@
+"""Monte Carlo shadow flux on the GPU against the oracle (needs a B200).
+
+The GPU and the oracle draw the same rand_r sample points (the reference's seeds and order),
+form the same FP32 rays and run the same FP32 Moller-Trumbore test; the GPU finds candidate
+triangles through a BVH, the oracle tests them all. Bar: identical shadow counts for at least
+99.9 % of the (face, phase) entries, never more than one sample apart, and flux factors equal
+to 1e-12 where the counts agree (the sun direction uses CUDA's cos / sin)."""
+from __future__ import annotations
+
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+
+def _counts(F, c6, nmonte):
+    lit = c6 > 1e-9
+    k = np.zeros_like(F)
+    k[lit] = (1.0 - F[lit] / c6[lit]) * nmonte
+    return np.round(k).astype(int), lit
+
+
+def _c6(n, za, tt):
+    phi = ((np.arange(tt) + 0.5) / tt) * 2.0 * np.pi + np.pi
+    s = np.stack([np.cos(-za) * np.sin(phi), np.cos(-za) * np.cos(phi), np.full(tt, np.sin(-za))], 1)
+    return n @ s.T
+
+
+def _compare(G, O_, c6, nmonte):
+    kg, lit = _counts(G, c6, nmonte)
+    ko, _ = _counts(O_, c6, nmonte)
+    same = kg == ko
+    assert same.mean() >= 0.999, same.mean()
+    assert np.abs(kg - ko).max() <= 1
+    np.testing.assert_allclose(G[same], O_[same], rtol=1e-12, atol=1e-12)
+    return kg[lit].sum()
+
+
+@pytest.mark.parametrize("nlevel,depth,za,tt,nmonte", [(3, 0.3, 0.2, 12, 32), (4, 0.15, 0.6, 6, 16)])
+def test_shadow_flux_matches_oracle(ctx, N, O, nlevel, depth, za, tt, nmonte):
+    from dsmc_suite_b200 import workloads as W
+    spot, facet = W.cratered_mesh(nlevel, depth=depth)
+    n = N.mesh_normals(spot, facet)["normal"]
+    G = ctx.shadow_flux(spot, facet, n, za, tt, nmonte)
+    O_ = O.shadow_flux(spot, facet, n, za, tt, nmonte)
+    shadowed = _compare(G, O_, _c6(n, za, tt), nmonte)
+    assert shadowed > 0
+
+
+def test_deep_bvh_on_a_large_mesh(ctx, N, O):
+    """20,480 faces: a tree of more levels than the small meshes; one phase, 4 samples."""
+    from dsmc_suite_b200 import workloads as W
+    spot, facet = W.cratered_mesh(5, craters=40, depth=0.25, width=0.15)
+    n = N.mesh_normals(spot, facet)["normal"]
+    G = ctx.shadow_flux(spot, facet, n, 0.4, 1, 4)
+    O_ = O.shadow_flux(spot, facet, n, 0.4, 1, 4, nthreads=32)
+    assert _compare(G, O_, _c6(n, 0.4, 1), 4) > 0
+
+
+def test_cli_raytrace_writes_the_flux_file(N, O, tmp_path, built):
+    from dsmc_suite_b200 import workloads as W
+    spot, facet = W.cratered_mesh(3, depth=0.3)
+    (tmp_path / "v.dat").write_text("".join("%.17g %.17g %.17g\n" % tuple(p) for p in spot))
+    (tmp_path / "f.dat").write_text("".join("%d %d %d\n" % tuple(f + 1) for f in facet))
+    cli = ROOT / "dsmc_suite_b200" / "bin" / "dsmc_suite"
+    r = subprocess.run([str(cli), "raytrace", "-m", str(tmp_path / "v.dat"), "-f",
+                        str(tmp_path / "f.dat"), "--npoint", str(len(spot)), "--nface",
+                        str(len(facet)), "--za", "10", "--tt", "8", "--nmonte", "20", "-o",
+                        str(tmp_path / "r")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "Flux written to" in r.stdout
+    vals = (tmp_path / "r_flux.dat").read_text().split()
+    assert vals[:2] == [str(len(facet)), "8"]
+    F = np.array(vals[2:], dtype=np.float64).reshape(len(facet), 8)
+    n = N.mesh_normals(spot, facet)["normal"]
+    O_ = O.shadow_flux(spot, facet, n, 10 / 180 * np.pi, 8, 20)
+    assert np.mean(np.abs(F - O_) <= 1e-7) >= 0.999

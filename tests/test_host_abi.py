@@ -225,7 +225,7 @@ def test_cli_usage_and_out_of_scope_commands(built):
     r = subprocess.run([str(cli)], capture_output=True, text=True)
     assert r.returncode == 1 and "dsmc-adv" in r.stdout
     r = subprocess.run([str(cli), "raytrace"], capture_output=True, text=True)
-    assert r.returncode == 1 and "not part of this build" in r.stderr
+    assert r.returncode == 1 and "requires -m" in r.stderr
     r = subprocess.run([str(cli), "bogus"], capture_output=True, text=True)
     assert r.returncode == 1 and "Unknown command" in r.stderr
 
