@@ -51,10 +51,12 @@ def args_parse():
                     help="launch shape block,blocks_per_sm,steps_per_launch,launches_per_graph")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", choices=["solve", "batch", "serve", "collisional"], default="solve",
+    ap.add_argument("--mode", choices=["solve", "batch", "serve", "collisional", "thermal",
+                                       "raytrace"], default="solve",
                     help="solve: one config-1 solve per step (default); batch: the 64-instance "
                          "batch; serve: the Poisson request stream; collisional: the config-2 "
-                         "two-phase solve")
+                         "two-phase solve; thermal: the surface thermal model; raytrace: the "
+                         "shadow-flux model on a synthetic cratered mesh")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--seconds", type=float, default=60.0, help="serve: arrival window [s]")
     ap.add_argument("--sample", type=float, default=0.05,
@@ -513,10 +515,87 @@ def run_collisional_mode(a):
     print(json.dumps(line), flush=True)
 
 
+def run_thermal_mode(a):
+    """The thermal column model (36 x 72 columns, Ceres defaults): wall time per solve through
+    dsmc_thermal_solve_host (host flux and profile set-up, upload, kernel, download), next to the
+    reference's own thermal_solve (oracle/_ref, OpenMP on all host cores) when it is built."""
+    from dsmc_suite_b200 import _native as N, Context
+    from oracle import oracle as O
+    tp = N.ThermalParams.default()
+    with Context(0) as ctx:
+        for _ in range(a.warmup):
+            ctx.thermal(36, 72, tp)
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            T, h = ctx.thermal(36, 72, tp)
+        gpu_s = (time.perf_counter() - t0) / a.steps
+    To, _ = O.thermal(36, 72, tp)
+    line = {"metric": "thermal solves/s", "value": 1.0 / gpu_s, "unit": "solves/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": gpu_s * 1e3,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"thermal column model, 36 x 72 columns x {h} depth points x "
+                                   f"{tp.n_substep} steps, Ceres defaults, analytic flux"},
+            "max_abs_diff_vs_oracle_K": float(np.abs(T - To).max()),
+            "identical_cells_vs_oracle": float(np.mean(T == To))}
+    so = ROOT / "oracle" / "_ref" / "libdsmcref.so"
+    if so.exists():
+        import ctypes
+        R = ctypes.CDLL(str(so))
+        g = N.SphericalGrid(ftd=36, ffd=72, hd=1, temperature=N.ptr(np.zeros((36, 72))))
+        cores = os.cpu_count() or 1
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        saved = os.dup(1)
+        os.dup2(devnull, 1)          # the reference prints progress lines
+        try:
+            t0 = time.perf_counter()
+            R.thermal_solve(ctypes.byref(g), ctypes.byref(tp), None, cores)
+            ref_s = time.perf_counter() - t0
+        finally:
+            os.dup2(saved, 1)
+            os.close(devnull)
+        line["cpu_baseline"] = {"value": 1.0 / ref_s, "unit": "solves/s", "cores": cores,
+                                "kind": "reference", "sample": "one full solve, reference build"}
+    print(json.dumps(line), flush=True)
+
+
+def run_raytrace_mode(a):
+    """The shadow-flux model on a synthetic cratered icosphere (81,920 faces, 24 phases, 50
+    samples per face): shadow rays per second through dsmc_shadow_flux_host, BVH build and
+    transfers included."""
+    from dsmc_suite_b200 import _native as N, Context
+    from dsmc_suite_b200 import workloads as W
+    spot, facet = W.cratered_mesh(6, craters=64, depth=0.2, width=0.12)
+    n = N.mesh_normals(spot, facet)["normal"]
+    tt, nm, za = 24, 50, 12.3 / 180 * np.pi
+    with Context(0) as ctx:
+        for _ in range(a.warmup):
+            F = ctx.shadow_flux(spot, facet, n, za, tt, nm)
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            F = ctx.shadow_flux(spot, facet, n, za, tt, nm)
+        dt = (time.perf_counter() - t0) / a.steps
+    phi = ((np.arange(tt) + 0.5) / tt) * 2.0 * np.pi + np.pi
+    sun = np.stack([np.cos(-za) * np.sin(phi), np.cos(-za) * np.cos(phi), np.full(tt, np.sin(-za))], 1)
+    rays = int((n @ sun.T >= 0).sum()) * nm
+    line = {"metric": "shadow rays/s", "value": rays / dt, "unit": "rays/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": dt * 1e3,
+            "higher_is_better": True, "dtype": "fp32 rays, f64 sampling", "data": "synthetic",
+            "config": {"workload": f"cratered icosphere, {len(facet)} faces, {tt} phases x {nm} "
+                                   f"samples, {rays} rays per solve"},
+            "shadowed_fraction": float(1.0 - F.sum() / np.clip(n @ sun.T, 0, None).sum()),
+            "cpu_baseline": None,
+            "cpu_baseline_note": "the reference traces with Intel Embree, not installed here"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = args_parse()
     if a.impl == "reference":
         return run_reference_arm(a)
+    if a.mode == "thermal":
+        return run_thermal_mode(a)
+    if a.mode == "raytrace":
+        return run_raytrace_mode(a)
     if a.mode == "collisional":
         return run_collisional_mode(a)
     if a.mode == "batch":
