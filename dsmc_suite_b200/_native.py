@@ -212,6 +212,7 @@ SIGNATURES = [
                                           _DP, C.POINTER(C.c_int)]),
     ("thermal_params_default", None, [C.POINTER(ThermalParams)]),
     ("thermal_solve", None, [C.POINTER(SphericalGrid), C.POINTER(ThermalParams), _DP, C.c_int]),
+    ("dsmc_last_kernel_ms", C.c_int, [_P, _DP]),
     ("dsmc_shadow_flux_host", C.c_int, [_P, C.c_int, _DP, C.c_int, _I32P, _DP, C.c_double,
                                         C.c_int, C.c_int, _DP]),
     ("mesh_load", C.POINTER(Mesh), [C.c_char_p, C.c_char_p, C.c_int, C.c_int]),

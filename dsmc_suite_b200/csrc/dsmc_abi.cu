@@ -35,6 +35,7 @@ struct dsmc_ctx {
     unsigned long long *stats = nullptr;
     dsmc::FastEngine *fast = nullptr;
     long long last_launches = 0;
+    double last_kernel_ms = 0.0;     // device time of the last thermal / shadow-flux kernel
     char err[512] = {0};
 };
 
@@ -552,8 +553,10 @@ int dsmc_thermal_solve_host(dsmc_ctx *c, int ftd, int ffd, const ThermalParams *
     // absorbed flux (the reference's analytic one when none is given, thermal_model.c:130-148),
     // the initial profile from radiative balance (:172-181), and the coefficients of the
     // tridiagonal system shared by every column (:230-244, forward sweep of :80-103)
-    const size_t ncol = static_cast<size_t>(st.ncol);
-    std::vector<double> F(ncol), qT0(ncol * h), cpv(h), piv(h);
+    // one host block [|F| | initial T | c'_i | pivots] and one device block for everything
+    const size_t ncol = static_cast<size_t>(st.ncol), hh = static_cast<size_t>(h);
+    std::vector<double> in(2 * ncol + 2 * hh);
+    double *F = in.data(), *T_init = F + ncol, *cpv = T_init + ncol, *piv = cpv + hh;
     const double Si = CONST_SOLAR_1AU * (1.0 / tp->distance_AU) * (1.0 / tp->distance_AU);
     const double dF = Si * (1.0 - tp->albedo);
     for (int td = 0; td < ftd; td++)
@@ -568,10 +571,7 @@ int dsmc_thermal_solve_host(dsmc_ctx *c, int ftd, int ffd, const ThermalParams *
             }
             F[td * ffd + fd] = fabs(f);
         }
-    for (size_t k = 0; k < ncol; k++) {
-        const double T_init = F[k] > 0 ? pow(F[k] / CONST_SIGMA, 0.25) : 100.0;
-        for (int d = 0; d < h; d++) qT0[static_cast<size_t>(d) * ncol + k] = T_init;
-    }
+    for (size_t k = 0; k < ncol; k++) T_init[k] = F[k] > 0 ? pow(F[k] / CONST_SIGMA, 0.25) : 100.0;
     cpv[0] = 0.0 / 1.0;
     piv[0] = 1.0;
     for (int i = 1; i < h; i++) {
@@ -581,27 +581,36 @@ int dsmc_thermal_solve_host(dsmc_ctx *c, int ftd, int ffd, const ThermalParams *
         piv[i] = bi - ai * cpv[i - 1];
         cpv[i] = ci / piv[i];
     }
-    struct Bufs {
-        void *p[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-        ~Bufs() { for (void *q : p) if (q) cudaFree(q); }
-    } b;
-    const size_t prof = ncol * h * sizeof(double);
-    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[0], ncol * sizeof(double)));
-    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[1], h * sizeof(double)));
-    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[2], h * sizeof(double)));
-    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[3], prof));
-    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[4], prof));
-    DSMC_CUDA_TRY(c, cudaMalloc(&b.p[5], ncol * sizeof(double)));
-    double *dF_ = static_cast<double *>(b.p[0]), *dcp = static_cast<double *>(b.p[1]);
-    double *dpiv = static_cast<double *>(b.p[2]), *dq = static_cast<double *>(b.p[3]);
-    double *ddp = static_cast<double *>(b.p[4]), *dT = static_cast<double *>(b.p[5]);
-    DSMC_CUDA_TRY(c, cudaMemcpyAsync(dF_, F.data(), ncol * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    DSMC_CUDA_TRY(c, cudaMemcpyAsync(dcp, cpv.data(), h * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    DSMC_CUDA_TRY(c, cudaMemcpyAsync(dpiv, piv.data(), h * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    DSMC_CUDA_TRY(c, cudaMemcpyAsync(dq, qT0.data(), prof, cudaMemcpyHostToDevice, c->stream));
-    DSMC_CUDA_TRY(c, dsmc::launch_thermal(st, dF_, dcp, dpiv, dq, ddp, dT, c->stream));
-    DSMC_CUDA_TRY(c, cudaMemcpyAsync(T_surface, dT, ncol * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    const size_t words = in.size() + 2 * ncol * hh + ncol;
+    if (words > (size_t(1) << 30)) return fail(c, DSMC_ERR_INVALID, "thermal grid too large (%zu doubles)", words);
+    void *blk = nullptr;
+    DSMC_CUDA_TRY(c, cudaMallocAsync(&blk, words * sizeof(double), c->stream));
+    double *d_in = static_cast<double *>(blk);
+    double *dq = d_in + in.size(), *ddp = dq + ncol * hh, *dT = ddp + ncol * hh;
+    cudaError_t e = cudaMemcpyAsync(d_in, in.data(), in.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (e == cudaSuccess) e = cudaEventCreate(&ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev[1]);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], c->stream);
+    if (e == cudaSuccess)
+        e = dsmc::launch_thermal(st, d_in, d_in + ncol, d_in + 2 * ncol, d_in + 2 * ncol + hh, dq, ddp, dT,
+                                 c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(T_surface, dT, ncol * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(blk, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    float ms = 0.f;
+    if (e == cudaSuccess && cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) c->last_kernel_ms = ms;
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    if (e != cudaSuccess) return fail(c, DSMC_ERR_CUDA, "thermal solve: %s", cudaGetErrorString(e));
+    return DSMC_OK;
+}
+
+int dsmc_last_kernel_ms(const dsmc_ctx *c, double *ms) {
+    if (!c || !ms) return DSMC_ERR_INVALID;
+    *ms = c->last_kernel_ms;
     return DSMC_OK;
 }
 
@@ -618,7 +627,7 @@ int dsmc_shadow_flux_host(dsmc_ctx *c, int npoint, const double *spot, int nface
     if (rc != DSMC_OK) return rc;
     long long overflows = 0;
     DSMC_CUDA_TRY(c, dsmc::shadow_flux(npoint, spot, nface, facet, face_normal, za, tt, nmonte, F,
-                                       c->stream, &overflows));
+                                       c->stream, &overflows, &c->last_kernel_ms));
     if (overflows) return fail(c, DSMC_ERR_INVALID, "BVH deeper than the traversal stack");
     return DSMC_OK;
 }

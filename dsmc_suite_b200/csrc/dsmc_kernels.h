@@ -39,17 +39,17 @@ struct ThermalSetup {
     double R, k_over_dr, a_last;
     double p[5], LH[5], tran_p, tran_LH, mmol;
 };
-// flux [ncol] = |F|; cp, piv [h]; qT [h][ncol] holds the initial profiles and receives the final
-// ones; dp [h][ncol] scratch; T_surface [ncol].
-cudaError_t launch_thermal(const ThermalSetup &s, const double *flux, const double *cp,
-                           const double *piv, double *qT, double *dp, double *T_surface,
-                           cudaStream_t stream);
+// flux, T_init [ncol] = |F| and the initial (uniform) column temperature; cp, piv [h]; qT, dp
+// [h][ncol] scratch (qT ends with the final profiles); T_surface [ncol].
+cudaError_t launch_thermal(const ThermalSetup &s, const double *flux, const double *T_init,
+                           const double *cp, const double *piv, double *qT, double *dp,
+                           double *T_surface, cudaStream_t stream);
 
 // Monte Carlo shadow flux (kernel_raytrace.cu): builds the BVH of the mesh on the host, traces
 // on `stream` and copies F [nface][tt] back (synchronous). *overflows counts traversal-stack
 // overflows (0 for meshes below 2^24 faces).
 cudaError_t shadow_flux(int npoint, const double *spot, int nface, const int *facet,
                         const double *normal, double za, int tt, int nmonte, double *F_host,
-                        cudaStream_t stream, long long *overflows);
+                        cudaStream_t stream, long long *overflows, double *kernel_ms);
 
 }  // namespace dsmc

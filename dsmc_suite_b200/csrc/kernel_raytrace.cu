@@ -275,7 +275,7 @@ __global__ void shadow_kernel(const ShadowArgs a) {
 
 cudaError_t shadow_flux(int npoint, const double *spot, int nface, const int *facet,
                         const double *normal, double za, int tt, int nmonte, double *F_host,
-                        cudaStream_t stream, long long *overflows) {
+                        cudaStream_t stream, long long *overflows, double *kernel_ms) {
     std::vector<float> V(3 * static_cast<size_t>(npoint));
     for (size_t k = 0; k < V.size(); k++) V[k] = static_cast<float>(spot[k]);
     Builder bld(V, facet, nface);
@@ -325,14 +325,24 @@ cudaError_t shadow_flux(int npoint, const double *spot, int nface, const int *fa
     a.overflow = static_cast<int *>(b.p[6]);
     const int block = 128;
     const long long threads = static_cast<long long>(nfc) * tt;
+    struct Events {
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~Events() { for (cudaEvent_t x : e) if (x) cudaEventDestroy(x); }
+    } ev;
+    if ((e = cudaEventCreate(&ev.e[0])) != cudaSuccess || (e = cudaEventCreate(&ev.e[1])) != cudaSuccess ||
+        (e = cudaEventRecord(ev.e[0], stream)) != cudaSuccess)
+        return e;
     shadow_kernel<<<static_cast<unsigned>((threads + block - 1) / block), block, 0, stream>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ev.e[1], stream)) != cudaSuccess) return e;
     int ovf = 0;
     if ((e = cudaMemcpyAsync(F_host, b.p[5], nF * sizeof(double), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(&ovf, b.p[6], sizeof(int), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(stream)) != cudaSuccess)
         return e;
     if (overflows) *overflows = ovf;
+    float ms = 0.f;
+    if (kernel_ms && cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]) == cudaSuccess) *kernel_ms = ms;
     return cudaSuccess;
 }
 

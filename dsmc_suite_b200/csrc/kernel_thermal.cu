@@ -27,6 +27,7 @@ struct ThermalArgs {
     double R, k_over_dr, a_last;     // CN weight, k/dr, lower coefficient of the bottom row
     double p[5], LH[5], tran_p, tran_LH, mmol;
     const double *flux;              // [ncol] absorbed flux |F|
+    const double *T_init;            // [ncol] initial column temperature
     const double *cp, *piv;          // [h] forward-sweep c'_i and pivots b_i - a_i c'_(i-1)
     double *qT, *dp;                 // [h][ncol] profiles and forward-sweep d'_i
     double *T_surface;               // [ncol]
@@ -45,10 +46,13 @@ __device__ double surface_balance(const ThermalArgs &a, double T, double F, doub
 __global__ void thermal_column_kernel(const ThermalArgs a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.ncol) return;
-    const int h = a.h, n = a.ncol;
+    const int h = a.h;
+    const long long n = a.ncol;
     double *qT = a.qT + c, *dp = a.dp + c;   // element d at [d * n]
     const double F = a.flux[c];
     const double R = a.R, w0 = 1.0 - 2.0 * R;
+    const double T_init = a.T_init[c];
+    for (int d = 0; d < h; d++) qT[d * n] = T_init;
     for (int step = 0; step < a.n_sub; step++) {
         const double oT = qT[1 * n];
         double T0 = 50.0, T1 = 300.0;
@@ -94,9 +98,9 @@ __global__ void thermal_column_kernel(const ThermalArgs a) {
 
 }  // namespace
 
-cudaError_t launch_thermal(const ThermalSetup &s, const double *flux, const double *cp,
-                           const double *piv, double *qT, double *dp, double *T_surface,
-                           cudaStream_t stream) {
+cudaError_t launch_thermal(const ThermalSetup &s, const double *flux, const double *T_init,
+                           const double *cp, const double *piv, double *qT, double *dp,
+                           double *T_surface, cudaStream_t stream) {
     ThermalArgs a{};
     a.ncol = s.ncol;
     a.h = s.h;
@@ -112,12 +116,13 @@ cudaError_t launch_thermal(const ThermalSetup &s, const double *flux, const doub
     a.tran_LH = s.tran_LH;
     a.mmol = s.mmol;
     a.flux = flux;
+    a.T_init = T_init;
     a.cp = cp;
     a.piv = piv;
     a.qT = qT;
     a.dp = dp;
     a.T_surface = T_surface;
-    const int block = 64;
+    const int block = 32;   // one warp per block: the 81 warps of a 36 x 72 grid spread over 81 SMs
     thermal_column_kernel<<<(s.ncol + block - 1) / block, block, 0, stream>>>(a);
     return cudaGetLastError();
 }

@@ -188,6 +188,12 @@ class Context:
                                                       N.ptr(T), C.byref(h)), "thermal")
         return T, h.value
 
+    def last_kernel_ms(self) -> float:
+        """Device time of the last thermal or shadow-flux kernel on this context."""
+        ms = C.c_double()
+        self._check(self._lib.dsmc_last_kernel_ms(self.h, C.byref(ms)), "last_kernel_ms")
+        return ms.value
+
     # shadow flux ------------------------------------------------------------------------------
     def shadow_flux(self, spot: np.ndarray, facet: np.ndarray, normal: np.ndarray, za: float,
                     tt: int = 24, nmonte: int = 50) -> np.ndarray:

@@ -234,6 +234,10 @@ const char *dsmc_noalloc_last_error(void);
 int dsmc_thermal_solve_host(dsmc_ctx *ctx, int ftd, int ffd, const ThermalParams *tp,
                             const double *flux, double *T_surface, int *h_depth);
 
+/* Device time [ms] of the kernel of the last dsmc_thermal_solve_host / dsmc_shadow_flux_host
+ * call on this context (CUDA events around the launch; host set-up and copies excluded). */
+int dsmc_last_kernel_ms(const dsmc_ctx *ctx, double *ms);
+
 /* ---- Shadow flux ------------------------------------------------------------------------------ */
 /* Replaces the Embree loop of the reference's ray tracer (src/raytracer/shadow_maker.c:198-238):  */
 /* for rotation phase t in [0, tt) and face f, F[f][t] = (1 - shadowed / nmonte) (s . n_f), 0 when  */
