@@ -400,6 +400,10 @@ __device__ __forceinline__ void horizon_add(const FastInst &I, int td, int fd, f
 
 // Launch from the current surface position (ballistic.c:156-181; config: flux-weighted
 // Maxwell-Boltzmann). Returns false when the reference's launch-speed escape test fires.
+// kCfg: every instance of the launch is a config-model problem, so the reference-model branches
+// of the event code are compiled out (shorter code on the path that high-gravity bodies take every
+// few hundred steps).
+template <bool kCfg>
 __device__ bool launch(const FastArgs &a, long long i, const FastInst &I, Hot &h, StatAcc &st,
                        float local_T, float thi, float fi) {
     const dsmc_params &p = I.p;
@@ -411,7 +415,7 @@ __device__ bool launch(const FastArgs &a, long long i, const FastInst &I, Hot &h
     double s[3];
     get_pos(h, s);
     float v[3];
-    if (p.model == DSMC_MODEL_REFERENCE) {
+    if (!kCfg && p.model == DSMC_MODEL_REFERENCE) {
         const float KF = 2.0f * kPiF * static_cast<float>(p.Radii) * fabsf(cosf(thi)) / static_cast<float>(p.P);
         int idx = local_T >= 220.0f ? 20 : static_cast<int>(ceilf(local_T / 10.0f)) - 2;
         idx = idx < 0 ? 0 : (idx >= 23 ? 22 : idx);
@@ -487,13 +491,14 @@ __device__ void enter_cell_near(const FastInst &I, Hot &h, Bounds &b) {
 // Start of a hop (ballistic.c:124-181, advanced.c:271-333): weight and life checks, the
 // reference freeze scan, the launch and the starting cell. Returns 0 when the particle flies,
 // else its fate.
+template <bool kCfg>
 __device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h, Bounds &b,
                        StatAcc &st, float thi, float fi, float local_T, bool first) {
     const dsmc_params &p = I.p;
     const float W = weight(I, h);
     if (W < static_cast<float>(p.w_min)) return DSMC_FATE_PHOTOLYSED;
     if (p.life_step_cap > 0 && h.steps >= p.life_step_cap) return DSMC_FATE_STEP_CAP;
-    if (p.model == DSMC_MODEL_REFERENCE) {
+    if (!kCfg && p.model == DSMC_MODEL_REFERENCE) {
         const int ftd = p.ftd, ffd = p.ffd;
         int td, fd;
         ref_index(thi, fi, ftd, ffd, td, fd);
@@ -541,7 +546,7 @@ __device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h
             local_T = static_cast<float>(T[td * ffd + fd]);
         }
     }
-    if (!launch(a, i, I, h, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
+    if (!launch<kCfg>(a, i, I, h, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
     // the running weight restarts from its exact value at every launch (and at every cell
     // change): points of the particle's own trajectory, so results do not depend on where
     // kernel launches begin or end
@@ -564,10 +569,11 @@ __device__ __forceinline__ void angles_of_f(const Hot &h, float &thi, float &fi)
 
 // Landing (ballistic.c:239-264): polar deposit (reference) or night freeze-out / day-side
 // re-emission point (config). Returns 0 to start a new hop, else the fate.
+template <bool kCfg>
 __device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &local_T) {
     const dsmc_params &p = I.p;
     int td, fd;
-    if (p.model == DSMC_MODEL_REFERENCE) {
+    if (!kCfg && p.model == DSMC_MODEL_REFERENCE) {
         angles_of_f(h, thi, fi);
         ref_index(thi, fi, p.ftd, p.ffd, td, fd);
         if (td <= 1 || td >= p.ftd - 2) {
@@ -701,6 +707,7 @@ __device__ __forceinline__ int find_inst(const FastArgs &a, unsigned long long w
 // Fill an empty slot with the next particle from the queue and launch it; particles that end
 // at their first launch are finished here and the next one is taken. Returns false when the
 // queue is empty.
+template <bool kCfg>
 __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, StatAcc &st) {
     for (;;) {
         const unsigned long long w = grab_work(a.ctr);
@@ -731,7 +738,7 @@ __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, St
         float thi, fi, local_T = 0.0f;
         double col_p = 0.0;
         double s[3];
-        if (p.model == DSMC_MODEL_REFERENCE) {
+        if (!kCfg && p.model == DSMC_MODEL_REFERENCE) {
             const bool adv = p.runner == DSMC_RUNNER_ADVANCED;
             if (adv) col_p = rng.raw(0) / kTwo32;
             const int o = adv ? 1 : 0;
@@ -776,7 +783,7 @@ __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, St
                 I.t.ttime[6 * I.t.out_cap + slot] = local_T;
             }
         }
-        const int fate = hop_top(a, i, I, h, b, st, thi, fi, local_T, true);
+        const int fate = hop_top<kCfg>(a, i, I, h, b, st, thi, fi, local_T, true);
         if (fate == 0) return true;
         finish(a, i, I, h, st, fate);
     }
@@ -830,7 +837,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
         h.ci = ci;
         h.run_w = run_w;
     } else {
-        alive = start_next(a, i, h, b, st);
+        alive = start_next<kLean>(a, i, h, b, st);
     }
     int cur = -1, flags = 0, half_ffd = 0, life_cap = 0, hop_cap = 0, col_ht = 0, nbins = 0;
     float GM = 0.f, dt = 0.f, c1 = 0.f, c2 = 0.f, rl2 = 0.f, re2 = 0.f, cday = 0.f, sx = 0.f,
@@ -944,12 +951,12 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
                 fate = DSMC_FATE_STEP_CAP;
             } else {
                 float thi, fi, local_T = 0.f;
-                fate = land(*I, h, thi, fi, local_T);
-                if (fate == 0) fate = hop_top(a, i, *I, h, b, st, thi, fi, local_T, false);
+                fate = land<kLean>(*I, h, thi, fi, local_T);
+                if (fate == 0) fate = hop_top<kLean>(a, i, *I, h, b, st, thi, fi, local_T, false);
             }
             if (fate) {
                 finish(a, i, *I, h, st, fate);
-                alive = start_next(a, i, h, b, st);
+                alive = start_next<kLean>(a, i, h, b, st);
             }
         }
     }
