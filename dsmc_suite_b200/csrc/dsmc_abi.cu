@@ -36,6 +36,8 @@ struct dsmc_ctx {
     dsmc::FastEngine *fast = nullptr;
     long long last_launches = 0;
     double last_kernel_ms = 0.0;     // device time of the last thermal / shadow-flux kernel
+    void *scratch = nullptr;          // grow-only device scratch of the thermal solve
+    size_t scratch_bytes = 0;
     char err[512] = {0};
 };
 
@@ -144,6 +146,7 @@ int dsmc_ctx_destroy(dsmc_ctx *c) {
     free_tables(c);
     free_outputs(c);
     if (c->stats) cudaFree(c->stats);
+    if (c->scratch) cudaFree(c->scratch);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return DSMC_OK;
@@ -583,9 +586,15 @@ int dsmc_thermal_solve_host(dsmc_ctx *c, int ftd, int ffd, const ThermalParams *
     }
     const size_t words = in.size() + 2 * ncol * hh + ncol;
     if (words > (size_t(1) << 30)) return fail(c, DSMC_ERR_INVALID, "thermal grid too large (%zu doubles)", words);
-    void *blk = nullptr;
-    DSMC_CUDA_TRY(c, cudaMallocAsync(&blk, words * sizeof(double), c->stream));
-    double *d_in = static_cast<double *>(blk);
+    if (c->scratch_bytes < words * sizeof(double)) {
+        DSMC_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if (c->scratch) cudaFree(c->scratch);
+        c->scratch = nullptr;
+        c->scratch_bytes = 0;
+        DSMC_CUDA_TRY(c, cudaMalloc(&c->scratch, words * sizeof(double)));
+        c->scratch_bytes = words * sizeof(double);
+    }
+    double *d_in = static_cast<double *>(c->scratch);
     double *dq = d_in + in.size(), *ddp = dq + ncol * hh, *dT = ddp + ncol * hh;
     cudaError_t e = cudaMemcpyAsync(d_in, in.data(), in.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -598,7 +607,6 @@ int dsmc_thermal_solve_host(dsmc_ctx *c, int ftd, int ffd, const ThermalParams *
     if (e == cudaSuccess) e = cudaEventRecord(ev[1], c->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(T_surface, dT, ncol * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-    cudaFreeAsync(blk, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     float ms = 0.f;
     if (e == cudaSuccess && cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) c->last_kernel_ms = ms;
