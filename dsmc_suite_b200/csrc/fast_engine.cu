@@ -569,6 +569,32 @@ __device__ __forceinline__ void angles_of_f(const Hot &h, float &thi, float &fi)
 
 // Landing (ballistic.c:239-264): polar deposit (reference) or night freeze-out / day-side
 // re-emission point (config). Returns 0 to start a new hop, else the fate.
+// Face of the icosphere containing unit direction n, from the FP32 tables: the nearest of the 20
+// base-face centroids, then one corner-cut test triple per subdivision level (the FP64 descent of
+// locate_face on FP32 copies).
+__device__ __forceinline__ int locate_face_f(const float4 *tab, int nlevel, const float n[3]) {
+    int node = 0;
+    float best = -2.0f;
+#pragma unroll 4
+    for (int f = 0; f < 20; f++) {
+        const float4 c = __ldg(tab + f);
+        const float d = c.x * n[0] + c.y * n[1] + c.z * n[2];
+        if (d > best) { best = d; node = f; }
+    }
+    int offset = 0, width = 20;
+    for (int level = 0; level < nlevel; level++) {
+        const float4 *pl = tab + 20 + 3 * (offset + node);
+        const float4 a = __ldg(pl), b = __ldg(pl + 1), c = __ldg(pl + 2);
+        const int child = (a.x * n[0] + a.y * n[1] + a.z * n[2] > 0.0f) ? 0
+                        : (b.x * n[0] + b.y * n[1] + b.z * n[2] > 0.0f) ? 1
+                        : (c.x * n[0] + c.y * n[1] + c.z * n[2] > 0.0f) ? 2 : 3;
+        node = node * 4 + child;
+        offset += width;
+        width *= 4;
+    }
+    return node;
+}
+
 template <bool kCfg>
 __device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &local_T) {
     const dsmc_params &p = I.p;
@@ -600,7 +626,8 @@ __device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &loc
     const double nd[3] = {n[0], n[1], n[2]};
     const double s[3] = {nd[0] * p.Radii, nd[1] * p.Radii, nd[2] * p.Radii};
     set_pos(h, s);
-    local_T = static_cast<float>(I.t.face_T[locate_face(I.t, nd)]);
+    const int face = I.face_f ? locate_face_f(I.face_f, I.t.nlevel, n) : locate_face(I.t, nd);
+    local_T = static_cast<float>(I.t.face_T[face]);
     return 0;
 }
 
@@ -1097,6 +1124,41 @@ int launch_mode(const std::vector<dsmc_params> &ps, const std::vector<DevTables>
 
 }  // namespace
 
+namespace {
+
+// FP32 copies of the icosphere's base-face centroids and corner-cut planes, as float4 (xyz, 0):
+// [0, 20) centroids, then 3 planes per subdivision node. Built on the device from the problem's
+// FP64 tables.
+__global__ void face_tables_kernel(const double *cent, const double *planes, int nnode, float4 *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 20) {
+        out[i] = make_float4(static_cast<float>(cent[3 * i]), static_cast<float>(cent[3 * i + 1]),
+                             static_cast<float>(cent[3 * i + 2]), 0.0f);
+    } else if (i < 20 + 3 * nnode) {
+        const double *q = planes + 3 * static_cast<long long>(i - 20);   // node (i-20)/3, plane (i-20)%3
+        out[i] = make_float4(static_cast<float>(q[0]), static_cast<float>(q[1]), static_cast<float>(q[2]), 0.0f);
+    }
+}
+
+}  // namespace
+
+size_t face_floats_for(int nlevel) {
+    const size_t nnode = static_cast<size_t>(20 * ((1 << (2 * nlevel)) - 1) / 3);
+    return 4 * (20 + 3 * nnode);
+}
+
+size_t face_table_floats(const dsmc_params &p, const DevTables &t) {
+    if (p.model != DSMC_MODEL_CONFIG || !t.base_centroid || !t.split_planes || t.nlevel < 0) return 0;
+    return face_floats_for(t.nlevel);
+}
+
+cudaError_t build_face_tables(const DevTables &t, float4 *out, cudaStream_t stream) {
+    const int nnode = 20 * ((1 << (2 * t.nlevel)) - 1) / 3;
+    const int n = 20 + 3 * nnode;
+    face_tables_kernel<<<(n + 127) / 128, 128, 0, stream>>>(t.base_centroid, t.split_planes, nnode, out);
+    return cudaGetLastError();
+}
+
 cudaError_t FastEngine::ensure_slots(int num_sms) {
     // one wave: as many blocks per SM as can be resident together
     variant_ = pick_variant(block, blocks_per_sm, mode_);
@@ -1157,13 +1219,20 @@ cudaError_t FastEngine::upload_instances(const std::vector<dsmc_params> &ps,
                                          cudaStream_t stream) {
     const int n = static_cast<int>(ps.size());
     // boundary tables, one block per instance: rb2 [hd+1], sbs [ftd+1], lonb [2*(ffd+1)]
-    std::vector<size_t> off(n);
+    // and, for config-model instances, the FP32 icosphere tables (face_table_floats)
+    std::vector<size_t> off(n), foff(n, 0);
     size_t total = 0;
     for (int k = 0; k < n; k++) {
         off[k] = total;
         total += (ps[k].hd + 1) + (ps[k].ftd + 1);
         total = (total + 1) & ~static_cast<size_t>(1);  // float2 alignment
         total += 2 * (ps[k].ffd + 1);
+        const size_t ff = face_table_floats(ps[k], ts[k]);
+        if (ff) {
+            total = (total + 3) & ~static_cast<size_t>(3);   // float4 alignment
+            foff[k] = total;
+            total += ff;
+        }
     }
     std::vector<float> tab(total, 0.0f);
     std::vector<FastInst> inst(n);
@@ -1209,6 +1278,7 @@ cudaError_t FastEngine::upload_instances(const std::vector<dsmc_params> &ps,
         I.rb2 = reinterpret_cast<const float *>(off[k]);
         I.sbs = reinterpret_cast<const float *>(off[k] + (p.hd + 1));
         I.lonb = reinterpret_cast<const float2 *>(lo);
+        I.face_f = foff[k] ? reinterpret_cast<const float4 *>(foff[k]) : nullptr;
         base += counts[k];
     }
     cudaError_t e;
@@ -1230,11 +1300,15 @@ cudaError_t FastEngine::upload_instances(const std::vector<dsmc_params> &ps,
         I.rb2 = d_tab_ + reinterpret_cast<size_t>(I.rb2);
         I.sbs = d_tab_ + reinterpret_cast<size_t>(I.sbs);
         I.lonb = reinterpret_cast<const float2 *>(d_tab_ + reinterpret_cast<size_t>(I.lonb));
+        if (I.face_f) I.face_f = reinterpret_cast<const float4 *>(d_tab_ + reinterpret_cast<size_t>(I.face_f));
     }
     if ((e = cudaMemcpyAsync(d_tab_, tab.data(), total * sizeof(float), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return e;
     if ((e = cudaMemcpyAsync(d_inst_, inst.data(), n * sizeof(FastInst), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return e;
+    for (int k = 0; k < n; k++)
+        if (inst[k].face_f && (e = build_face_tables(ts[k], const_cast<float4 *>(inst[k].face_f), stream)) != cudaSuccess)
+            return e;
     ninst_ = n;
     // the host staging vectors die here: wait for the copies
     return cudaStreamSynchronize(stream);
@@ -1409,7 +1483,8 @@ cudaError_t FastEngine::serve_append(const dsmc_params &p, const DevTables &t, l
                                      int *index, cudaStream_t upload, cudaStream_t compute) {
     if (ninst_ >= ninst_cap_ || !d_stats_) return cudaErrorMemoryAllocation;
     if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767 || n < 0 || n > (1ll << 32)) return cudaErrorInvalidValue;
-    const size_t need = serve_table_floats(p);
+    const size_t need = serve_table_floats(p, face_table_floats(p, t) ? t.nlevel : -1);
+    const size_t base_need = static_cast<size_t>(p.hd + 1) + (p.ftd + 1) + 1 + 2 * static_cast<size_t>(p.ffd + 1);
     void *d_tab = nullptr;
     cudaError_t e = pool_ ? cudaMallocFromPoolAsync(&d_tab, need * sizeof(float), pool_, upload)
                           : cudaMallocAsync(&d_tab, need * sizeof(float), upload);
@@ -1423,10 +1498,16 @@ cudaError_t FastEngine::serve_append(const dsmc_params &p, const DevTables &t, l
         return e;
     }
     host.work_base = static_cast<long long>(serve_total_);
+    float4 *face = nullptr;
+    if (face_table_floats(p, t)) {
+        face = reinterpret_cast<float4 *>(static_cast<float *>(d_tab) + ((base_need + 3) & ~static_cast<size_t>(3)));
+        host.face_f = face;
+    }
     // The new descriptor lies beyond the instances the kernels in flight can see; it is written
     // on the upload stream while they run, and published on the compute stream after them.
     if ((e = cudaMemcpyAsync(d_tab, tab.data(), need * sizeof(float), cudaMemcpyHostToDevice, upload)) != cudaSuccess ||
         (e = cudaMemcpyAsync(d_inst_ + ninst_, &host, sizeof host, cudaMemcpyHostToDevice, upload)) != cudaSuccess ||
+        (face && (e = build_face_tables(t, face, upload)) != cudaSuccess) ||
         (e = cudaStreamSynchronize(upload)) != cudaSuccess) {
         cudaFreeAsync(d_tab, upload);
         return e;
@@ -1473,8 +1554,11 @@ void FastEngine::serve_close(cudaStream_t stream) {
     inst_tabs_.clear();
 }
 
-size_t FastEngine::serve_table_floats(const dsmc_params &p) {
-    return static_cast<size_t>(p.hd + 1) + (p.ftd + 1) + 1 + 2 * static_cast<size_t>(p.ffd + 1);
+size_t FastEngine::serve_table_floats(const dsmc_params &p, int nlevel) {
+    // boundary tables, then (config model, icosphere of nlevel levels) the FP32 face tables
+    const size_t base = static_cast<size_t>(p.hd + 1) + (p.ftd + 1) + 1 + 2 * static_cast<size_t>(p.ffd + 1);
+    if (p.model != DSMC_MODEL_CONFIG || nlevel < 0) return base;
+    return ((base + 3) & ~static_cast<size_t>(3)) + face_floats_for(nlevel);
 }
 
 size_t FastEngine::serve_fixed_bytes(int max_instances) const {

@@ -24,7 +24,14 @@ struct FastInst {
     long long pid_begin;     // particle id of the first particle
     float c_day;             // h / lifetime / ln 2 (W = W0 * 2^(-c_day * n_day))
     float r_land2, r_esc2;   // Radii^2, max_height^2
+    const float4 *face_f;    // FP32 icosphere tables (config model), or nullptr: FP64 descent
 };
+
+// FP32 icosphere tables of an instance (floats; 0 when the problem has no icosphere) and their
+// construction on the device from the problem's FP64 tables.
+size_t face_floats_for(int nlevel);
+size_t face_table_floats(const dsmc_params &p, const DevTables &t);
+cudaError_t build_face_tables(const DevTables &t, float4 *out, cudaStream_t stream);
 
 // Structure-of-arrays particle slots.
 struct Slots {
@@ -134,7 +141,9 @@ public:
     const unsigned long long *serve_stats_rows() const { return d_stats_; }
     int serve_instances() const { return ninst_; }
     int serve_capacity() const { return ninst_cap_; }
-    static size_t serve_table_floats(const dsmc_params &p);
+    // floats of an instance's table block: boundary tables, plus the FP32 icosphere tables of a
+    // config-model problem with an icosphere of nlevel levels (nlevel < 0: none)
+    static size_t serve_table_floats(const dsmc_params &p, int nlevel);
     void serve_set_pool(cudaMemPool_t pool) { pool_ = pool; }
     void serve_close(cudaStream_t stream);   // frees every instance's boundary tables
     size_t serve_fixed_bytes(int max_instances) const;

@@ -7,7 +7,8 @@
 // plugin loaded into a process whose allocation calls are intercepted or budgeted. They can
 // still pass device buffers they already hold. This entry point therefore allocates nothing: the
 // scratch the fast kernel needs (the resident particle slots, the instance descriptor, the cell
-// boundary tables, the work-queue counters and the reference-model speed table) lives in one
+// boundary tables, the work-queue counters, the reference-model speed table and the FP32
+// icosphere tables) lives in one
 // file-scope device array of fixed size, which every GPU that loads the library holds until the
 // process exits.
 #include <cstdio>
@@ -44,7 +45,9 @@ constexpr size_t kVtOff = kCtrOff + kCtrBytes;
 constexpr size_t kVtBytes = round_up(23 * 1000 * sizeof(double));
 constexpr size_t kCntOff = kVtOff + kVtBytes;
 constexpr size_t kCntBytes = round_up(23 * sizeof(int));
-constexpr size_t kScratchBytes = kCntOff + kCntBytes;   // about 4.6 MB
+constexpr size_t kFaceOff = kCntOff + kCntBytes;       // FP32 icosphere tables, up to 6 levels
+constexpr size_t kFaceBytes = round_up(4 * (20 + 3 * 27300) * sizeof(float));
+constexpr size_t kScratchBytes = kFaceOff + kFaceBytes;   // about 5.9 MB
 
 // The scratch itself. In host code `g_scratch` names a host-side stand-in, not the device
 // memory: its device address comes from cudaGetSymbolAddress, once per device.
@@ -145,6 +148,13 @@ extern "C" int dsmc_solve_fast_noalloc(const dsmc_params *p, const dsmc_surface 
     e = dsmc::fast_fill_instance(*p, t, pid_begin, n, reinterpret_cast<float *>(base + kTabOff),
                                  kTabFloats, inst_host, tab_host);
     if (e != cudaSuccess) return fail_cuda("instance tables", e);
+    if (!ref) {
+        // the FP32 copies of the icosphere tables the fast kernel descends (same as the engine)
+        float4 *face = reinterpret_cast<float4 *>(base + kFaceOff);
+        reinterpret_cast<dsmc::FastInst *>(inst_host)->face_f = face;
+        e = dsmc::build_face_tables(t, face, stream);
+        if (e != cudaSuccess) return fail_cuda("icosphere tables", e);
+    }
     e = cudaMemcpyAsync(base + kInstOff, inst_host, sizeof inst_host, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(base + kTabOff, tab_host, sizeof tab_host, cudaMemcpyHostToDevice, stream);

@@ -323,7 +323,8 @@ int dsmc_server_submit(dsmc_server *s, const dsmc_params *p, const dsmc_surface 
         if ((rc = drain_rounds(s)) != DSMC_OK) return rc;
         if ((rc = open_queue(s)) != DSMC_OK) return rc;
     }
-    const size_t tab = dsmc::FastEngine::serve_table_floats(*p) * sizeof(float);
+    const size_t tab = dsmc::FastEngine::serve_table_floats(
+                           *p, p->model == DSMC_MODEL_CONFIG ? surf->nlevel : -1) * sizeof(float);
     const size_t est = dsmc::problem_bytes(p, surf, col) + tab;
     if (s->in_use + est > s->budget) {
         s->rejected++;
