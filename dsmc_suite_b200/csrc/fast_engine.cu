@@ -596,7 +596,8 @@ __device__ __forceinline__ int locate_face_f(const float4 *tab, int nlevel, cons
 }
 
 template <bool kCfg>
-__device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &local_T) {
+__device__ int land(const FastArgs &a, long long i, const FastInst &I, Hot &h, float &thi, float &fi,
+                    float &local_T) {
     const dsmc_params &p = I.p;
     int td, fd;
     if (!kCfg && p.model == DSMC_MODEL_REFERENCE) {
@@ -626,7 +627,25 @@ __device__ int land(const FastInst &I, Hot &h, float &thi, float &fi, float &loc
     const double nd[3] = {n[0], n[1], n[2]};
     const double s[3] = {nd[0] * p.Radii, nd[1] * p.Radii, nd[2] * p.Radii};
     set_pos(h, s);
-    const int face = I.face_f ? locate_face_f(I.face_f, I.t.nlevel, n) : locate_face(I.t, nd);
+    int face;
+    if (I.face_f) {
+        // hops are short next to the face size on high-gravity bodies: try the face of the last
+        // launch point first (three sign tests), descend the tree only when the point left it
+        const int last = a.s.face[i];
+        const int nnode = 20 * ((1 << (2 * I.t.nlevel)) - 1) / 3;
+        const float4 *ed = I.face_f + 20 + 3 * nnode + 3 * last;
+        bool inside = last >= 0;
+        if (inside) {
+            const float4 e0 = __ldg(ed), e1 = __ldg(ed + 1), e2 = __ldg(ed + 2);
+            inside = (e0.x * n[0] + e0.y * n[1] + e0.z * n[2] >= 0.0f) &
+                     (e1.x * n[0] + e1.y * n[1] + e1.z * n[2] >= 0.0f) &
+                     (e2.x * n[0] + e2.y * n[1] + e2.z * n[2] >= 0.0f);
+        }
+        face = inside ? last : locate_face_f(I.face_f, I.t.nlevel, n);
+        a.s.face[i] = face;
+    } else {
+        face = locate_face(I.t, nd);
+    }
     local_T = static_cast<float>(I.t.face_T[face]);
     return 0;
 }
@@ -781,6 +800,7 @@ __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, St
             local_T = static_cast<float>(I.t.T_map[td * p.ffd + fd]);
         } else {
             const int f = pick_face(I.t, rng.raw(0) / kTwo32);
+            a.s.face[i] = f;
             double u1 = rng.raw(1) / kTwo32, u2 = rng.raw(2) / kTwo32;
             col_p = rng.raw(3) / kTwo32;
             if (u1 + u2 > 1.0) { u1 = 1.0 - u1; u2 = 1.0 - u2; }
@@ -978,7 +998,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
                 fate = DSMC_FATE_STEP_CAP;
             } else {
                 float thi, fi, local_T = 0.f;
-                fate = land<kLean>(*I, h, thi, fi, local_T);
+                fate = land<kLean>(a, i, *I, h, thi, fi, local_T);
                 if (fate == 0) fate = hop_top<kLean>(a, i, *I, h, b, st, thi, fi, local_T, false);
             }
             if (fate) {
@@ -1127,16 +1147,30 @@ int launch_mode(const std::vector<dsmc_params> &ps, const std::vector<DevTables>
 namespace {
 
 // FP32 copies of the icosphere's base-face centroids and corner-cut planes, as float4 (xyz, 0):
-// [0, 20) centroids, then 3 planes per subdivision node. Built on the device from the problem's
-// FP64 tables.
-__global__ void face_tables_kernel(const double *cent, const double *planes, int nnode, float4 *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// [0, 20) centroids, then 3 planes per subdivision node, then per leaf face the normals of the 3
+// planes through the origin and its edges, turned so that the face's cone is on their positive
+// side (a point lies in face f iff its direction is on the positive side of all three). Built on
+// the device from the problem's FP64 tables.
+__global__ void face_tables_kernel(const double *cent, const double *planes, const double *verts,
+                                   int nnode, int nface, float4 *out) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long long np = 20 + 3ll * nnode;
     if (i < 20) {
         out[i] = make_float4(static_cast<float>(cent[3 * i]), static_cast<float>(cent[3 * i + 1]),
                              static_cast<float>(cent[3 * i + 2]), 0.0f);
-    } else if (i < 20 + 3 * nnode) {
-        const double *q = planes + 3 * static_cast<long long>(i - 20);   // node (i-20)/3, plane (i-20)%3
+    } else if (i < np) {
+        const double *q = planes + 3 * (i - 20);   // node (i-20)/3, plane (i-20)%3
         out[i] = make_float4(static_cast<float>(q[0]), static_cast<float>(q[1]), static_cast<float>(q[2]), 0.0f);
+    } else if (i < np + 3ll * nface) {
+        const long long f = (i - np) / 3;
+        const int e = static_cast<int>((i - np) % 3);
+        const double *v = verts + 9 * f;
+        const double *p = v + 3 * e, *q = v + 3 * ((e + 1) % 3);
+        double c[3] = {p[1] * q[2] - p[2] * q[1], p[2] * q[0] - p[0] * q[2], p[0] * q[1] - p[1] * q[0]};
+        const double m[3] = {v[0] + v[3] + v[6], v[1] + v[4] + v[7], v[2] + v[5] + v[8]};
+        if (c[0] * m[0] + c[1] * m[1] + c[2] * m[2] < 0.0)
+            for (int k = 0; k < 3; k++) c[k] = -c[k];
+        out[i] = make_float4(static_cast<float>(c[0]), static_cast<float>(c[1]), static_cast<float>(c[2]), 0.0f);
     }
 }
 
@@ -1144,18 +1178,23 @@ __global__ void face_tables_kernel(const double *cent, const double *planes, int
 
 size_t face_floats_for(int nlevel) {
     const size_t nnode = static_cast<size_t>(20 * ((1 << (2 * nlevel)) - 1) / 3);
-    return 4 * (20 + 3 * nnode);
+    const size_t nface = static_cast<size_t>(20) << (2 * nlevel);
+    return 4 * (20 + 3 * nnode + 3 * nface);
 }
 
 size_t face_table_floats(const dsmc_params &p, const DevTables &t) {
-    if (p.model != DSMC_MODEL_CONFIG || !t.base_centroid || !t.split_planes || t.nlevel < 0) return 0;
+    if (p.model != DSMC_MODEL_CONFIG || !t.base_centroid || !t.split_planes || !t.face_verts ||
+        t.nlevel < 0)
+        return 0;
     return face_floats_for(t.nlevel);
 }
 
 cudaError_t build_face_tables(const DevTables &t, float4 *out, cudaStream_t stream) {
     const int nnode = 20 * ((1 << (2 * t.nlevel)) - 1) / 3;
-    const int n = 20 + 3 * nnode;
-    face_tables_kernel<<<(n + 127) / 128, 128, 0, stream>>>(t.base_centroid, t.split_planes, nnode, out);
+    const int nface = 20 << (2 * t.nlevel);
+    const int n = 20 + 3 * nnode + 3 * nface;
+    face_tables_kernel<<<(n + 127) / 128, 128, 0, stream>>>(t.base_centroid, t.split_planes,
+                                                            t.face_verts, nnode, nface, out);
     return cudaGetLastError();
 }
 
@@ -1176,8 +1215,8 @@ cudaError_t FastEngine::ensure_slots(int num_sms) {
     if (slot_mem_) { cudaFree(slot_mem_); slot_mem_ = nullptr; }
     const long long S = want;
     // 4-byte fields: inst pid evt (3) + 15 vector floats + w0 nday steps hop cell run_cell
-    // hist_key hist_cnt pcol pthr ncol rest wcur (13) = 31 words; plus run_w (8-byte slot).
-    const size_t bytes = static_cast<size_t>(S) * (31 * 4 + 8) + 256;
+    // hist_key hist_cnt pcol pthr ncol rest wcur face (14) = 32 words; plus run_w (8-byte slot).
+    const size_t bytes = static_cast<size_t>(S) * (32 * 4 + 8) + 256;
     cudaError_t e = cudaMalloc(&slot_mem_, bytes);
     if (e != cudaSuccess) return e;
     char *b = static_cast<char *>(slot_mem_);
@@ -1204,6 +1243,7 @@ cudaError_t FastEngine::ensure_slots(int num_sms) {
     slots_.ncol = reinterpret_cast<int *>(take(4));
     slots_.rest = reinterpret_cast<float *>(take(4));
     slots_.wcur = reinterpret_cast<float *>(take(4));
+    slots_.face = reinterpret_cast<int *>(take(4));
     nslots_ = S;
     if (!d_ctr_) {
         if ((e = cudaMalloc(&d_ctr_, sizeof(FastCounters))) != cudaSuccess) return e;
@@ -1567,7 +1607,7 @@ size_t FastEngine::serve_fixed_bytes(int max_instances) const {
 }
 
 size_t fast_slot_bytes(long long nslots) {
-    return static_cast<size_t>(nslots) * (31 * 4 + 8) + 256;
+    return static_cast<size_t>(nslots) * (32 * 4 + 8) + 256;
 }
 
 size_t fast_inst_bytes() { return sizeof(FastInst); }
@@ -1649,6 +1689,7 @@ cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long ns
     s.ncol = reinterpret_cast<int *>(take(4));
     s.rest = reinterpret_cast<float *>(take(4));
     s.wcur = reinterpret_cast<float *>(take(4));
+    s.face = reinterpret_cast<int *>(take(4));
     cudaError_t e;
     FastCounters host{};
     host.total = static_cast<unsigned long long>(total);

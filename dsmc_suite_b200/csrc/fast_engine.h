@@ -52,6 +52,7 @@ struct Slots {
     int *ncol;
     float *rest;             // freeze waiting time (reference model)
     float *wcur;             // running weight (the hot loop's W between launches)
+    int *face;               // icosphere face of the last launch point (config model), -1 = none
 };
 
 // Device-side queue state. `total` and `ninst` live here rather than in the kernel arguments so

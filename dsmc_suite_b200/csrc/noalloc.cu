@@ -34,7 +34,7 @@ constexpr int kBlock = 128;                // threads per block: 256 blocks of 1
 constexpr size_t kTabFloats = 4096;        // (hd+1) + (ftd+1) + 2 (ffd+1) + 1 floats at most
 
 constexpr size_t kSlotOff = 0;
-constexpr size_t kSlotBytes = round_up(static_cast<size_t>(kSlots) * (31 * 4 + 8) + 256);
+constexpr size_t kSlotBytes = round_up(static_cast<size_t>(kSlots) * (32 * 4 + 8) + 256);
 constexpr size_t kInstOff = kSlotOff + kSlotBytes;
 constexpr size_t kInstBytes = round_up(sizeof(dsmc::FastInst));
 constexpr size_t kTabOff = kInstOff + kInstBytes;
@@ -46,8 +46,8 @@ constexpr size_t kVtBytes = round_up(23 * 1000 * sizeof(double));
 constexpr size_t kCntOff = kVtOff + kVtBytes;
 constexpr size_t kCntBytes = round_up(23 * sizeof(int));
 constexpr size_t kFaceOff = kCntOff + kCntBytes;       // FP32 icosphere tables, up to 6 levels
-constexpr size_t kFaceBytes = round_up(4 * (20 + 3 * 27300) * sizeof(float));
-constexpr size_t kScratchBytes = kFaceOff + kFaceBytes;   // about 5.9 MB
+constexpr size_t kFaceBytes = round_up(4 * (20 + 3 * 27300 + 3 * 81920) * sizeof(float));
+constexpr size_t kScratchBytes = kFaceOff + kFaceBytes;   // about 10.5 MB
 
 // The scratch itself. In host code `g_scratch` names a host-side stand-in, not the device
 // memory: its device address comes from cudaGetSymbolAddress, once per device.
