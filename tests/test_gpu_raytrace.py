@@ -79,3 +79,20 @@ def test_cli_raytrace_writes_the_flux_file(N, O, tmp_path, built):
     n = N.mesh_normals(spot, facet)["normal"]
     O_ = O.shadow_flux(spot, facet, n, 10 / 180 * np.pi, 8, 20)
     assert np.mean(np.abs(F - O_) <= 1e-7) >= 0.999
+
+
+def test_shadow_flux_edge_cases(ctx, N, O):
+    """A lone triangle (no occluder: the flux is the clipped cosine), one phase and one sample,
+    and the argument checks (vertex index out of range, no samples)."""
+    spot = np.array([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+    facet = np.array([[0, 1, 2]], dtype=np.int32)
+    n = N.mesh_normals(spot, facet)["normal"]
+    for tt, nm in ((1, 1), (16, 3)):
+        G = ctx.shadow_flux(spot, facet, n, 0.3, tt, nm)
+        c6 = _c6(n, 0.3, tt)
+        np.testing.assert_allclose(G, np.where(c6 < 0, 0.0, c6), rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(G, O.shadow_flux(spot, facet, n, 0.3, tt, nm), rtol=1e-12, atol=1e-15)
+    with pytest.raises(N.DsmcError):
+        ctx.shadow_flux(spot, np.array([[0, 1, 3]], dtype=np.int32), n, 0.3, 4, 4)
+    with pytest.raises(N.DsmcError):
+        ctx.shadow_flux(spot, facet, n, 0.3, 4, 0)

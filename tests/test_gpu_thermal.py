@@ -64,3 +64,24 @@ def test_cli_thermal_and_pipeline(N, O, tmp_path, built):
               "p_phase2_den.dat", "p_phase2_ttime.dat"):
         assert (tmp_path / f).exists(), f
     assert "PIPELINE COMPLETE" in r.stdout
+
+
+def test_thermal_edge_cases(ctx, N, O):
+    """Smallest grid and column (3 depth points), one step, a night-only flux, and the
+    argument checks."""
+    tp = N.ThermalParams.default()
+    tp.depth = 1e-6
+    tp.n_substep = 1
+    T, h = ctx.thermal(1, 2, tp)
+    To, ho = O.thermal(1, 2, tp)
+    assert h == ho == 3
+    _close(T, To)
+    flux = np.zeros((4, 6))
+    T, _ = ctx.thermal(4, 6, N.ThermalParams.default(), flux)
+    _close(T, O.thermal(4, 6, N.ThermalParams.default(), flux)[0])
+    bad = N.ThermalParams.default()
+    bad.n_substep = 0
+    with pytest.raises(N.DsmcError):
+        ctx.thermal(4, 6, bad)
+    with pytest.raises(N.DsmcError):
+        ctx.thermal(0, 6, N.ThermalParams.default())
