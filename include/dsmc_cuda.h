@@ -90,7 +90,8 @@ typedef struct dsmc_ctx dsmc_ctx;
  * the reference's FP64 arithmetic without FMA contraction, one atomic per deposited step.
  * FAST_FP32 keeps resident particle slots that refill from a work queue, pushes in FP32 with
  * two-sum compensated positions and velocities, tracks cells by comparisons, and aggregates
- * deposits in registers. FAST_FP64 is the same resident-slot engine with FP64 arithmetic. */
+ * deposits in registers. FAST_FP64 is reserved (not built; dsmc_run rejects it with
+ * DSMC_ERR_INVALID): the FP64 solve is PLAIN_FP64, which follows the reference's arithmetic. */
 enum dsmc_path { DSMC_PATH_PLAIN_FP64 = 0, DSMC_PATH_FAST_FP32 = 1, DSMC_PATH_FAST_FP64 = 2 };
 
 typedef struct dsmc_stats {
