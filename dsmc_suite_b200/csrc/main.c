@@ -52,7 +52,7 @@ static void print_usage(const char *prog)
     printf("  -d <den_file>      Density input file (for dsmc-adv)\n");
     printf("  -v <v_record_file> Velocity record file (for dsmc-adv)\n");
     printf("  -o <output_prefix> Output file prefix (default: output)\n");
-    printf("Environment: DSMC_DEVICE, DSMC_PATH (plain|fast32|fast64), DSMC_SEED\n");
+    printf("Environment: DSMC_DEVICE, DSMC_PATH (plain|fast32), DSMC_SEED\n");
 }
 
 int main(int argc, char *argv[])
