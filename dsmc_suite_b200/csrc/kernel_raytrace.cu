@@ -17,7 +17,9 @@
 #include "dsmc_kernels.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 namespace dsmc {
@@ -41,6 +43,7 @@ struct Builder {
     std::vector<int> idx;
     std::vector<float> cen, blo, bhi;   // per triangle centroid and box
     std::vector<BvhNode> nodes;
+    std::atomic<int> used{0};      // nodes handed out (subtrees are built by parallel threads)
 
     Builder(const std::vector<float> &v, const int *f, int n) : V(v), F(f), nface(n) {
         idx.resize(n);
@@ -78,10 +81,10 @@ struct Builder {
     }
 
     void build() {
-        nodes.clear();
-        nodes.reserve(2 * static_cast<size_t>(nface) + 1);
-        nodes.push_back(BvhNode{});
+        nodes.assign(2 * static_cast<size_t>(nface) + 1, BvhNode{});
+        used = 1;
         split(0, 0, nface, 0);
+        nodes.resize(static_cast<size_t>(used.load()));
     }
 
     void split(int node, int b, int e, int depth) {
@@ -144,13 +147,19 @@ struct Builder {
             std::nth_element(idx.data() + b, idx.data() + mid, idx.data() + e,
                              [&](int x, int y) { return cen[3 * x + axis] < cen[3 * y + axis]; });
         }
-        const int left = static_cast<int>(nodes.size());
-        nodes.push_back(BvhNode{});
-        nodes.push_back(BvhNode{});
+        const int left = used.fetch_add(2);
         nodes[node].first = left;
         nodes[node].count = 0;
-        split(left, b, mid, depth + 1);
-        split(left + 1, mid, e, depth + 1);
+        // the two subtrees touch disjoint index ranges and nodes: the upper levels of a large
+        // mesh are split across threads (at most 8)
+        if (depth < 3 && e - b > 20000) {
+            std::thread t([&] { split(left, b, mid, depth + 1); });
+            split(left + 1, mid, e, depth + 1);
+            t.join();
+        } else {
+            split(left, b, mid, depth + 1);
+            split(left + 1, mid, e, depth + 1);
+        }
     }
 };
 
