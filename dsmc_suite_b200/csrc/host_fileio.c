@@ -3,6 +3,7 @@
  * return NULL / -1 on a missing or short file instead of returning partly filled buffers. */
 #include "fileio.h"
 
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -156,4 +157,30 @@ int write_horizon_dat(const char *filename, const double *horizon, int ftd, int 
     const long n = (long)ftd * ffd;
     for (long i = 0; i < n; i++) fprintf(fp, "%9.6f\n", horizon[i]);
     return fclose(fp) == 0 ? 0 : -1;
+}
+
+/* Binary side-car of one run (not in the reference): the exact fixed-point density and horizon
+ * grids and the FP64 per-particle rows that _den.dat, _horizon.dat and _ttime.dat print rounded
+ * to 6 and 5 decimals. Little-endian, naturally aligned:
+ *   char magic[8] = "DSMCBIN1"; int32 ftd, ffd, hd, nrows; int64 totaln; double fixed_scale;
+ *   uint64 den[hd * ftd * ffd]   (the order of _den.dat)
+ *   uint64 horizon[ftd * ffd]    (the order of _horizon.dat)
+ *   double ttime[nrows * totaln] (the order of _ttime.dat)
+ * A grid value is count / fixed_scale, which is what the .dat files print. */
+int write_grids_bin(const char *filename, const uint64_t *den, const uint64_t *hor,
+                    const double *ttime, int ftd, int ffd, int hd, int nrows, int totaln,
+                    double fixed_scale)
+{
+    FILE *fp = open_or_report(filename, "wb");
+    if (!fp) return -1;
+    const int32_t dims[4] = {ftd, ffd, hd, nrows};
+    const int64_t n = totaln;
+    const size_t ncell = (size_t)hd * ftd * ffd, nh = (size_t)ftd * ffd,
+                 nt = (size_t)nrows * (totaln > 0 ? totaln : 0);
+    int ok = fwrite("DSMCBIN1", 1, 8, fp) == 8 && fwrite(dims, sizeof dims, 1, fp) == 1 &&
+             fwrite(&n, sizeof n, 1, fp) == 1 && fwrite(&fixed_scale, sizeof fixed_scale, 1, fp) == 1 &&
+             fwrite(den, sizeof *den, ncell, fp) == ncell &&
+             fwrite(hor, sizeof *hor, nh, fp) == nh &&
+             (nt == 0 || fwrite(ttime, sizeof *ttime, nt, fp) == nt);
+    return fclose(fp) == 0 && ok ? 0 : -1;
 }

@@ -79,6 +79,12 @@ static void write_grids(const char *prefix, const uint64_t *den, const uint64_t 
         write_horizon_dat(fname, hh, p->ftd, p->ffd);
         snprintf(fname, sizeof fname, "%s_ttime.dat", prefix);
         write_ttime_dat(fname, ttime, nrows, totaln);
+        if (env_int("DSMC_SIDECAR", 0)) {
+            snprintf(fname, sizeof fname, "%s_grids.bin", prefix);
+            if (write_grids_bin(fname, den, hor, ttime, p->ftd, p->ffd, p->hd, nrows, totaln,
+                                DSMC_FIXED_SCALE))
+                fprintf(stderr, "cannot write %s\n", fname);
+        }
     } else {
         fprintf(stderr, "out of host memory writing results\n");
     }

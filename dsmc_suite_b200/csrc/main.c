@@ -52,7 +52,8 @@ static void print_usage(const char *prog)
     printf("  -d <den_file>      Density input file (for dsmc-adv)\n");
     printf("  -v <v_record_file> Velocity record file (for dsmc-adv)\n");
     printf("  -o <output_prefix> Output file prefix (default: output)\n");
-    printf("Environment: DSMC_DEVICE, DSMC_PATH (plain|fast32), DSMC_SEED\n");
+    printf("  --bin              Also write <prefix>_grids.bin (exact grids, FP64 rows)\n");
+    printf("Environment: DSMC_DEVICE, DSMC_PATH (plain|fast32), DSMC_SEED, DSMC_SIDECAR\n");
 }
 
 int main(int argc, char *argv[])
@@ -80,6 +81,7 @@ int main(int argc, char *argv[])
         else if (!strcmp(argv[i], "--nface") && more) nface_mesh = atoi(argv[++i]);
         else if (!strcmp(argv[i], "--tt") && more) tt = atoi(argv[++i]);
         else if (!strcmp(argv[i], "--nmonte") && more) nmonte = atoi(argv[++i]);
+        else if (!strcmp(argv[i], "--bin")) setenv("DSMC_SIDECAR", "1", 1);
     }
     if (!strcmp(command, "dsmc")) {
         run_ballistic(totaln, temp_file, output_prefix, nthreads);

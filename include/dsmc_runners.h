@@ -5,8 +5,10 @@
  * files, solve on the GPU through include/dsmc_cuda.h and write the same output files:
  *   <prefix>_den.dat, <prefix>_horizon.dat, <prefix>_v_record.dat (ballistic), <prefix>_ttime.dat
  * nthreads is accepted for compatibility; the solve runs on one CUDA device (DSMC_DEVICE,
- * default 0). DSMC_PATH selects the kernel path (plain, fast32 or fast64; default plain) and
- * DSMC_SEED the Philox seed. On failure a message goes to stderr and no file is written. */
+ * default 0). DSMC_PATH selects the kernel path (plain or fast32; default plain) and DSMC_SEED
+ * the Philox seed. DSMC_SIDECAR=1 (the CLI's --bin) also writes <prefix>_grids.bin, the exact
+ * fixed-point grids and FP64 per-particle rows (layout in fileio.h / host_fileio.c). On failure
+ * a message goes to stderr and no file is written. */
 #ifndef DSMC_RUNNERS_H
 #define DSMC_RUNNERS_H
 

@@ -4,6 +4,8 @@
 #ifndef FILEIO_H
 #define FILEIO_H
 
+#include <stdint.h>
+
 #include "types.h"
 
 double *read_density_dat(const char *filename, int *ftd, int *ffd, int *hd, int has_hd);
@@ -18,5 +20,12 @@ int read_v_record_dat(const char *filename, double **v_record, int **td_list, in
 double *read_flux_dat(const char *filename, int *nface, int *tt);
 int write_flux_dat(const char *filename, const double *F, int nface, int tt);
 int write_horizon_dat(const char *filename, const double *horizon, int ftd, int ffd);
+
+/* Addition (no reference counterpart): the run's exact fixed-point grids and FP64 per-particle
+ * rows as one binary side-car, <prefix>_grids.bin, for comparisons the printed precision of the
+ * .dat files cannot settle. Layout in host_fileio.c; 0 on success, -1 on an I/O failure. */
+int write_grids_bin(const char *filename, const uint64_t *den, const uint64_t *hor,
+                    const double *ttime, int ftd, int ffd, int hd, int nrows, int totaln,
+                    double fixed_scale);
 
 #endif /* FILEIO_H */

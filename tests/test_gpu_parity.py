@@ -244,20 +244,31 @@ def test_fast_fp32_vs_plain_fp64(ctx, N, config_surface, model):
 
 
 def test_runner_files_match_oracle(N, O, tmp_path, built):
-    """The drop-in CLI (`dsmc_suite dsmc`) writes the reference's files; its density equals the
-    oracle's fixed-point grid to the printed precision and its velocity record to %f."""
+    """The drop-in CLI (`dsmc_suite dsmc --bin`) writes the reference's files; its density equals
+    the oracle's fixed-point grid to the printed precision and its velocity record to %f. The
+    binary side-car carries the exact grids and FP64 rows: the .dat text is those values printed,
+    and against the oracle they meet the plain path's bars (bit-identical cells, 1e-9 rows)."""
+    from dsmc_suite_b200.sidecar import read_grids_bin
     T = cold_T(N)
     (tmp_path / "T.dat").write_text("36\n72\n" + "".join(f"{x:.17g}\n" for x in T.ravel()))
     cli = ROOT / "dsmc_suite_b200" / "bin" / "dsmc_suite"
     n = 300
     r = subprocess.run([str(cli), "dsmc", "-n", str(n), "-T", str(tmp_path / "T.dat"), "-o",
-                        str(tmp_path / "g")], capture_output=True, text=True)
+                        str(tmp_path / "g"), "--bin"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert "Simulation complete" in r.stdout
     p = N.params_reference(N.RUNNER_BALLISTIC, 36, 72)
     o = O.run(p, N.SurfaceInputs(T_map=T), n, nthreads=1, v_record=True)
     den = np.array((tmp_path / "g_den.dat").read_text().split()[3:], dtype=np.float64)
     np.testing.assert_allclose(den, o["density"].ravel() / N.FIXED_SCALE, atol=1.5e-6)
+    g = read_grids_bin(tmp_path / "g_grids.bin")
+    assert (g["ftd"], g["ffd"], g["hd"], g["nrows"], g["totaln"]) == (36, 72, p.hd, 5, n)
+    lines = (tmp_path / "g_den.dat").read_text().split("\n")[3:-1]
+    assert lines == ["%9.6f" % x for x in g["density"] / g["fixed_scale"]]
+    assert np.mean(g["density"] == o["density"].ravel()) >= 0.999
+    assert np.mean(g["horizon"] == o["horizon"].ravel()) >= 0.99
+    same = np.all(np.isclose(g["ttime"], o["ttime"][:5], rtol=1e-9, atol=1e-6), axis=0)
+    assert same.mean() >= 0.995, same.mean()
     vr = (tmp_path / "g_v_record.dat").read_text().split()
     assert abs(int(vr[0]) - o["n_records"]) <= 0.01 * o["n_records"] + 1
     tt = np.array((tmp_path / "g_ttime.dat").read_text().split(), dtype=np.float64).reshape(5, n)

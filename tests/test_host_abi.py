@@ -220,6 +220,44 @@ def test_dat_formats_round_trip_and_bytes(N, tmp_path, golden):
     assert not L.read_temperature_dat(str(tmp_path / "missing.dat").encode(), C.byref(a), C.byref(b))
 
 
+def test_grids_side_car_round_trip(N, tmp_path):
+    """write_grids_bin + read_grids_bin give back the exact grids and FP64 rows; the values
+    count / fixed_scale print to the same text as write_density_dat / write_ttime_dat; a
+    truncated or foreign file is rejected."""
+    from dsmc_suite_b200.sidecar import read_grids_bin
+    L = N.lib()
+    u64 = C.POINTER(C.c_uint64)
+    L.write_grids_bin.argtypes = [C.c_char_p, u64, u64, C.POINTER(C.c_double)] + [C.c_int] * 5 + \
+        [C.c_double]
+    rng = np.random.default_rng(7)
+    ftd, ffd, hd, nrows, n = 3, 5, 4, 5, 11
+    den = rng.integers(0, 1 << 40, hd * ftd * ffd, dtype=np.uint64)
+    hor = rng.integers(0, 1 << 30, ftd * ffd, dtype=np.uint64)
+    tt = rng.normal(size=(nrows, n)) * 1e4
+    path = tmp_path / "r_grids.bin"
+    assert L.write_grids_bin(str(path).encode(), den.ctypes.data_as(u64), hor.ctypes.data_as(u64),
+                             N.ptr(tt), ftd, ffd, hd, nrows, n, N.FIXED_SCALE) == 0
+    g = read_grids_bin(path)
+    assert (g["ftd"], g["ffd"], g["hd"], g["nrows"], g["totaln"]) == (ftd, ffd, hd, nrows, n)
+    np.testing.assert_array_equal(g["density"], den)
+    np.testing.assert_array_equal(g["horizon"], hor)
+    np.testing.assert_array_equal(g["ttime"], tt)
+    L.write_density_dat.argtypes = [C.c_char_p, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int]
+    dd = np.ascontiguousarray(den / g["fixed_scale"])
+    assert L.write_density_dat(str(tmp_path / "r_den.dat").encode(), N.ptr(dd), ftd, ffd, hd) == 0
+    text = (tmp_path / "r_den.dat").read_text().split("\n")[3:-1]
+    assert text == ["%9.6f" % x for x in g["density"] / g["fixed_scale"]]
+    L.write_grids_bin(str(path).encode(), den.ctypes.data_as(u64), hor.ctypes.data_as(u64), None,
+                      ftd, ffd, hd, nrows, 0, N.FIXED_SCALE)
+    assert read_grids_bin(path)["ttime"].shape == (nrows, 0)
+    (tmp_path / "cut.bin").write_bytes(path.read_bytes()[:-8])
+    with pytest.raises(ValueError):
+        read_grids_bin(tmp_path / "cut.bin")
+    (tmp_path / "bad.bin").write_bytes(b"XXXXXXXX" + path.read_bytes()[8:])
+    with pytest.raises(ValueError):
+        read_grids_bin(tmp_path / "bad.bin")
+
+
 def test_cli_usage_and_out_of_scope_commands(built):
     cli = ROOT / "dsmc_suite_b200" / "bin" / "dsmc_suite"
     r = subprocess.run([str(cli)], capture_output=True, text=True)
