@@ -21,7 +21,7 @@ from pathlib import Path
 from .server import Server
 
 # (block, blocks_per_sm, steps_per_launch, launches_per_graph)
-CANDIDATES = [(b, bps, k, g) for b, bps in ((128, 3), (128, 4), (256, 2))
+CANDIDATES = [(b, bps, k, g) for b, bps in ((128, 3), (128, 4), (128, 5), (256, 2))
               for k in (1024, 2048, 4096) for g in (2, 4, 8)]
 
 

@@ -236,6 +236,7 @@ __device__ void enter_cell(const FastInst &I, Hot &h, Bounds &b, int cell) {
 // The particle left its cell: walk to the new cell one boundary at a time. Each move keeps the
 // shared boundary from the registers and loads only the next one, so a typical crossing costs
 // one table load. Same cells as track_shell / track_angles.
+template <bool kNoBg>
 __device__ __forceinline__ void move_cell(const FastInst &I, Hot &h, Bounds &b, float x, float y,
                                           float r2, float zz) {
     const int hd = I.p.hd, ftd = I.p.ftd, ffd = I.p.ffd;
@@ -291,7 +292,7 @@ __device__ __forceinline__ void move_cell(const FastInst &I, Hot &h, Bounds &b, 
     h.cell = cell;
     h.ci = (ht * ftd + td) * ffd + fd;
     h.W = h.w0 * exp2f(-I.c_day * static_cast<float>(h.nday));   // re-anchor the running weight
-    if (I.t.n_bg) {
+    if (!kNoBg && I.t.n_bg) {
         h.nsig = 0.0f;
         if (I.p.runner == DSMC_RUNNER_ADVANCED && ht < I.p.collide_ht_max && h.ci < I.t.n_bg_len)
             h.nsig = static_cast<float>(__ldg(I.t.n_bg + h.ci) * I.p.cross_section);
@@ -549,8 +550,8 @@ __device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h
     if (!launch<kCfg>(a, i, I, h, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
     // the running weight restarts from its exact value at every launch (and at every cell
     // change): points of the particle's own trajectory, so results do not depend on where
-    // kernel launches begin or end
-    h.W = weight(I, h);
+    // kernel launches begin or end (the launch changes neither w0 nor the day count)
+    h.W = W;
     if (first)
         enter_cell(I, h, b, cell_from_scratch(I, h.sh[0] + h.sl[0], h.sh[1] + h.sl[1], h.sh[2] + h.sl[2]));
     else
@@ -865,6 +866,11 @@ enum Flag { kRef = 1, kSkipFirst = 2, kCollide = 4, kHist = 8 };
 // collisions, so the reference-model, collision and histogram branches and the per-hop step
 // counter drop out of the loop. kMode 2: the same, with the collision branch kept (config-model
 // collisional instances).
+// The step loop runs in segments: an inner loop pushes the particle until an event (landing,
+// escape, cap) or the end of the launch's step budget, so the per-step path carries no instance
+// or restart checks, and the lean loops settle their step counters once per segment. This
+// structure measured 21 % faster than one flat loop over steps with the same arithmetic (and
+// bit-identical results).
 template <int kMaxThreads, int kMinBlocks, int kMode>
 __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const FastArgs a) {
     constexpr bool kLean = kMode != 0;
@@ -890,8 +896,6 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
     float GM = 0.f, dt = 0.f, c1 = 0.f, c2 = 0.f, rl2 = 0.f, re2 = 0.f, cday = 0.f, sx = 0.f,
           sy = 0.f, sz = 0.f, inv_bw = 0.f, fday = 0.f;
     const FastInst *I = nullptr;
-    float x = 0.f, y = 0.f, z = 0.f, r2 = 0.f;
-    bool fresh = true;
     int budget = a.K;
 
     while (alive && budget > 0) {
@@ -923,35 +927,37 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
             nbins = p.n_speed_bins;
             inv_bw = nbins > 0 ? static_cast<float>(1.0 / p.speed_bin_width) : 0.f;
         }
-        if (fresh) {
-            x = h.sh[0] + h.sl[0];
-            y = h.sh[1] + h.sl[1];
-            z = h.sh[2] + h.sl[2];
-            r2 = fmaf(x, x, fmaf(y, y, z * z));
-            fresh = false;
-        }
-        float d[3];
-        verlet_f32(h, x, y, z, r2, GM, dt, c1, c2, d);
-        budget--;
-        const int ii = kLean ? 1 : h.hop;
-        h.steps++;
-        if (!kLean) h.hop++;
-        st.steps++;
+        // One segment: steps until an event or the end of the launch's budget. The lean loop
+        // also stops at the life cap, so its step counters are settled once per segment.
+        float x = h.sh[0] + h.sl[0], y = h.sh[1] + h.sl[1], z = h.sh[2] + h.sl[2];
+        float r2 = fmaf(x, x, fmaf(y, y, z * z));
+        const int n = kLean ? min(budget, life_cap - h.steps) : budget;
+        int taken = 0;
         int event = 0;   // 1 landed (or hop cap), 2 escaped, 3 life cap
-        const float zz = z * fabsf(z);
-        const bool inside = (r2 > b.r2lo) & (r2 <= b.r2hi) & (zz > r2 * b.zlo) &
-                            (zz <= r2 * b.zhi) & (x * b.c0 - y * b.s0 > 0.0f) &
-                            (x * b.c1 - y * b.s1 <= 0.0f);
-        if (!inside) {
-            if (r2 <= rl2) {
-                event = 1;
-            } else if (r2 >= re2) {
-                event = 2;
-            } else {
-                move_cell(*I, h, b, x, y, r2, zz);
+        do {
+            float d[3];
+            verlet_f32(h, x, y, z, r2, GM, dt, c1, c2, d);
+            taken++;
+            const int ii = kLean ? 1 : h.hop;
+            if (!kLean) {
+                h.steps++;
+                h.hop++;
             }
-        }
-        if (!event) {
+            const float zz = z * fabsf(z);
+            const bool inside = (r2 > b.r2lo) & (r2 <= b.r2hi) & (zz > r2 * b.zlo) &
+                                (zz <= r2 * b.zhi) & (x * b.c0 - y * b.s0 > 0.0f) &
+                                (x * b.c1 - y * b.s1 <= 0.0f);
+            if (!inside) {
+                if (r2 <= rl2) {
+                    event = 1;
+                    break;
+                }
+                if (r2 >= re2) {
+                    event = 2;
+                    break;
+                }
+                move_cell<kMode == 1>(*I, h, b, x, y, r2, zz);
+            }
             const bool day = (!kLean && (flags & kRef)) ? ((h.cell & 0xff) < half_ffd)
                                                         : (fmaf(x, sx, fmaf(y, sy, z * sz)) > 0.0f);
             if (day) {
@@ -986,11 +992,18 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
                     }
                 }
             }
-            if (h.steps >= life_cap) event = 3;
-            else if (!kLean && h.hop >= hop_cap) event = 1;
+            if (!kLean) {
+                if (h.steps >= life_cap) event = 3;
+                else if (h.hop >= hop_cap) event = 1;
+            }
+        } while (!event && taken < n);
+        budget -= taken;
+        st.steps += taken;
+        if (kLean) {
+            h.steps += taken;
+            if (!event && h.steps >= life_cap) event = 3;
         }
         if (event) {
-            fresh = true;
             int fate = 0;
             if (event == 2) {
                 fate = DSMC_FATE_ESCAPED;
@@ -1107,19 +1120,22 @@ void (*kernel_variant(int variant, int mode))(FastArgs) {
         case 2: return by_mode<128, 3>(mode);
         case 3: return fast_kernel<128, 2, 0>;
         case 4: return by_mode<128, 4>(mode);
+        case 5: return by_mode<128, 5>(mode);
         default: return by_mode<256, 2>(mode);
     }
 }
 
 // Variant for a launch shape: blocks_per_sm names the register budget. The default (0) is the
-// fastest measured on B200: the lean loop fits 128 registers without spills (16 warps per SM),
-// the general loop needs 168 (12 warps per SM) to avoid them.
+// fastest measured on B200: the lean loop at 96 registers (20 warps per SM; ptxas reports 44 B of
+// spill stores) beats 128 registers without spills (16 warps) by 6 % and 80 registers (24
+// warps) by 3 %; the general loop needs 168 (12 warps per SM) to avoid spills.
 int pick_variant(int block, int blocks_per_sm, int mode) {
     if (block > 128) return blocks_per_sm >= 3 ? 1 : 0;
     if (blocks_per_sm == 2) return 3;
     if (blocks_per_sm == 3) return 2;
     if (blocks_per_sm == 4) return 4;
-    return mode == 1 ? 4 : 2;   // the collision loop (mode 2) fits 168 registers without spills
+    if (blocks_per_sm == 5) return 5;
+    return mode == 1 ? 5 : 2;   // the collision loop (mode 2) fits 168 registers without spills
 }
 
 // Loop mode of one instance (see fast_kernel): 1 lean, 2 lean with collisions, 0 general.
