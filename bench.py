@@ -461,6 +461,9 @@ def run_collisional_mode(a):
     t_phase1 = time.perf_counter() - t0
     col, p, S = prob.collision, prob.params, prob.surface
     ctx.setup(p, S, col)
+    if a.shape:
+        N.check(N.lib().dsmc_set_launch_shape(ctx.h, *[int(v) for v in a.shape.split(",")]),
+                "launch shape", ctx.h)
 
     def solve(path):
         ctx.zero()

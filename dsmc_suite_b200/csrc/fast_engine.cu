@@ -1126,16 +1126,17 @@ void (*kernel_variant(int variant, int mode))(FastArgs) {
 }
 
 // Variant for a launch shape: blocks_per_sm names the register budget. The default (0) is the
-// fastest measured on B200: the lean loop at 96 registers (20 warps per SM; ptxas reports 44 B of
-// spill stores) beats 128 registers without spills (16 warps) by 6 % and 80 registers (24
-// warps) by 3 %; the general loop needs 168 (12 warps per SM) to avoid spills.
+// fastest measured on B200 for each loop, although ptxas reports spills for all three: the lean
+// loop at 96 registers (20 warps per SM) beats 128 registers (16 warps) by 6 % and 80 (24 warps)
+// by 3 %; the collision loop at 96 beats 128 by 1.5 % and 168 (no spills, 12 warps) by 15 %;
+// the general loop at 128 beats 168 by 19 % and 96 by 18 %.
 int pick_variant(int block, int blocks_per_sm, int mode) {
     if (block > 128) return blocks_per_sm >= 3 ? 1 : 0;
     if (blocks_per_sm == 2) return 3;
     if (blocks_per_sm == 3) return 2;
     if (blocks_per_sm == 4) return 4;
     if (blocks_per_sm == 5) return 5;
-    return mode == 1 ? 5 : 2;   // the collision loop (mode 2) fits 168 registers without spills
+    return mode == 0 ? 4 : 5;
 }
 
 // Loop mode of one instance (see fast_kernel): 1 lean, 2 lean with collisions, 0 general.
