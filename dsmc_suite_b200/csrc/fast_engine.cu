@@ -30,6 +30,35 @@ __device__ __forceinline__ void accumulate(float &hi, float &lo, float b) {
     hi = t;
 }
 
+// Philox4x32-10 block of the generator's current counter, with the ten rounds kept as a loop: the
+// same words as Philox::next in a fraction of its code. The collision loop takes it in its event
+// paths (launch, start, collision), which run on single lanes: there it cuts ptxas' spill stores
+// from 416 B to 188 B and measured 7 % faster on config 2; the lean and general loops measured
+// 1-3 % slower with it and keep the unrolled rounds.
+__device__ __forceinline__ void philox_next_rolled(Philox &r) {
+    uint32_t c0 = r.pid, c1 = r.event, c2 = r.inst, c3 = 0u, a = r.k0, b = r.k1;
+#pragma unroll 1
+    for (int k = 0; k < 10; k++) {
+        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        c0 = hi1 ^ c1 ^ a;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ b;
+        c3 = lo0;
+        a += 0x9E3779B9u;
+        b += 0xBB67AE85u;
+    }
+    r.w[0] = c0; r.w[1] = c1; r.w[2] = c2; r.w[3] = c3;
+    r.event++;
+}
+
+// kRoll: the collision loop's choice of the rolled rounds (same random words either way).
+template <bool kRoll>
+__device__ __forceinline__ void philox_next(Philox &r) {
+    if (kRoll) philox_next_rolled(r);
+    else r.next();
+}
+
 // u in (0, 1): 24 random bits plus half an ulp, so 1 - u and u are never 0.
 __device__ __forceinline__ float unit_open(uint32_t w) {
     return (static_cast<float>(w >> 8) + 0.5f) * (1.0f / 16777216.0f);
@@ -416,14 +445,14 @@ __device__ __forceinline__ void horizon_add(const FastInst &I, int td, int fd, f
 // kCfg: every instance of the launch is a config-model problem, so the reference-model branches
 // of the event code are compiled out (shorter code on the path that high-gravity bodies take every
 // few hundred steps).
-template <bool kCfg>
+template <bool kCfg, bool kRoll>
 __device__ bool launch(const FastArgs &a, long long i, const FastInst &I, Hot &h, StatAcc &st,
                        float local_T, float thi, float fi) {
     const dsmc_params &p = I.p;
     Philox rng;
     rng.init(p.seed, p.instance, a.s.pid[i]);
     rng.event = a.s.evt[i];
-    rng.next();
+    philox_next<kRoll>(rng);
     a.s.evt[i] = rng.event;
     double s[3];
     get_pos(h, s);
@@ -504,7 +533,7 @@ __device__ void enter_cell_near(const FastInst &I, Hot &h, Bounds &b) {
 // Start of a hop (ballistic.c:124-181, advanced.c:271-333): weight and life checks, the
 // reference freeze scan, the launch and the starting cell. Returns 0 when the particle flies,
 // else its fate.
-template <bool kCfg>
+template <bool kCfg, bool kRoll>
 __device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h, Bounds &b,
                        StatAcc &st, float thi, float fi, float local_T, bool first) {
     const dsmc_params &p = I.p;
@@ -559,7 +588,7 @@ __device__ int hop_top(const FastArgs &a, long long i, const FastInst &I, Hot &h
             local_T = static_cast<float>(T[td * ffd + fd]);
         }
     }
-    if (!launch<kCfg>(a, i, I, h, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
+    if (!launch<kCfg, kRoll>(a, i, I, h, st, local_T, thi, fi)) return DSMC_FATE_ESCAPED;
     // the running weight restarts from its exact value at every launch (and at every cell
     // change): points of the particle's own trajectory, so results do not depend on where
     // kernel launches begin or end (the launch changes neither w0 nor the day count)
@@ -701,13 +730,14 @@ __device__ void finish(const FastArgs &a, long long i, const FastInst &I, Hot &h
 }
 
 // A collision against a partner drawn from the cell's fitted speed CDF (advanced.c:374-396).
+template <bool kRoll>
 __device__ void collide(const FastArgs &a, long long i, const FastInst &I, Hot &h, long long pidx) {
     const dsmc_params &p = I.p;
     const DevTables &t = I.t;
     Philox rng;
     rng.init(p.seed, p.instance, a.s.pid[i]);
     rng.event = a.s.evt[i];
-    rng.next();
+    philox_next<kRoll>(rng);
     const double *coef = t.cdf_coef + DSMC_CDF_STRIDE * pidx;
     const double *box = t.cdf_box + 4 * pidx;
     double v[3];
@@ -724,7 +754,7 @@ __device__ void collide(const FastArgs &a, long long i, const FastInst &I, Hot &
         float d2[3], om[3];
         unit_sphere_f(unit_open(rng.w[1]), unit_open(rng.w[2]), d2);
         if (p.redraw_col_threshold) col_p = rng.raw(3) / kTwo32;
-        rng.next();
+        philox_next<kRoll>(rng);
         unit_sphere_f(unit_open(rng.w[0]), unit_open(rng.w[1]), om);
         double g2 = 0.0, vcm[3];
         for (int k = 0; k < 3; k++) {
@@ -766,7 +796,7 @@ __device__ __forceinline__ int find_inst(const FastArgs &a, unsigned long long w
 // Fill an empty slot with the next particle from the queue and launch it; particles that end
 // at their first launch are finished here and the next one is taken. Returns false when the
 // queue is empty.
-template <bool kCfg>
+template <bool kCfg, bool kRoll>
 __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, StatAcc &st) {
     for (;;) {
         const unsigned long long w = grab_work(a.ctr);
@@ -782,7 +812,7 @@ __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, St
         h.inst = ii;
         Philox rng;
         rng.init(p.seed, p.instance, pid);
-        rng.next();
+        philox_next<kRoll>(rng);
         h.w0 = 1.0f;
         h.nday = 0;
         h.steps = 0;
@@ -843,7 +873,7 @@ __device__ bool start_next(const FastArgs &a, long long i, Hot &h, Bounds &b, St
                 I.t.ttime[6 * I.t.out_cap + slot] = local_T;
             }
         }
-        const int fate = hop_top<kCfg>(a, i, I, h, b, st, thi, fi, local_T, true);
+        const int fate = hop_top<kCfg, kRoll>(a, i, I, h, b, st, thi, fi, local_T, true);
         if (fate == 0) return true;
         finish(a, i, I, h, st, fate);
     }
@@ -902,7 +932,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
         h.ci = ci;
         h.run_w = run_w;
     } else {
-        alive = start_next<kLean>(a, i, h, b, st);
+        alive = start_next<kLean, kMode == 2>(a, i, h, b, st);
     }
     int cur = -1, flags = 0, half_ffd = 0, life_cap = 0, hop_cap = 0, col_ht = 0, nbins = 0;
     float GM = 0.f, dt = 0.f, c1 = 0.f, c2 = 0.f, rl2 = 0.f, re2 = 0.f, cday = 0.f, sx = 0.f,
@@ -984,7 +1014,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
                         const int ht = h.cell >> 16, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
                         const long long pidx = (static_cast<long long>(td) * I->p.ffd + fd) * I->p.hd + ht;
                         if (ht < col_ht && __ldg(I->t.cdf_valid + pidx)) {
-                            collide(a, i, *I, h, pidx);
+                            collide<kMode == 2>(a, i, *I, h, pidx);
                             collided = true;
                         }
                     }
@@ -1024,11 +1054,11 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
             } else {
                 float thi, fi, local_T = 0.f;
                 fate = land<kLean>(a, i, *I, h, thi, fi, local_T);
-                if (fate == 0) fate = hop_top<kLean>(a, i, *I, h, b, st, thi, fi, local_T, false);
+                if (fate == 0) fate = hop_top<kLean, kMode == 2>(a, i, *I, h, b, st, thi, fi, local_T, false);
             }
             if (fate) {
                 finish(a, i, *I, h, st, fate);
-                alive = start_next<kLean>(a, i, h, b, st);
+                alive = start_next<kLean, kMode == 2>(a, i, h, b, st);
             }
         }
     }
