@@ -150,6 +150,17 @@ def cpu_oracle_rate(N, seconds: float, nthreads: int, n_hint: int | None = None)
     return r["total_steps"] / dt, n_hint, r["total_steps"], dt
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (first `model name` of /proc/cpuinfo), or "unknown"."""
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def reference_binary_rate(seconds: float, nthreads: int):
     """The unmodified reference binary (oracle/_ref/dsmc_suite, compiled from the reference's
     own sources) on its own reference-model workload: `dsmc -n N -t cores` on the synthetic
@@ -203,7 +214,8 @@ def run_reference_arm(a):
             "data": "synthetic", "config": dict(CONFIG, solver="CPU oracle port of the reference "
                                                 "algorithm, OpenMP over particles"),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
-                             "sample": f"{n} particles of the same workload per step"},
+                             "sample": f"{n} particles of the same workload per step",
+                             "cpu_model": cpu_model()},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     refbin = reference_binary_rate(per_step, cores)
@@ -800,6 +812,12 @@ def main():
         refbin = reference_binary_rate(a.cpu_seconds, cores)
         if refbin:
             line["cpu_baseline"]["reference_binary"] = refbin
+        # one thread, a quarter of the sample time: the per-core rate the OpenMP figure scales
+        r1, n1, s1, d1 = cpu_oracle_rate(N, a.cpu_seconds / 4, 1)
+        line["cpu_baseline"]["single_thread"] = {
+            "value": r1, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"{n1} particles, {s1} particle-steps in {d1:.1f} s"}
+        line["cpu_baseline"]["cpu_model"] = cpu_model()
 
     if rank == 0:
         print(json.dumps(line), flush=True)
