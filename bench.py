@@ -62,11 +62,20 @@ def args_parse():
     ap.add_argument("--sample", type=float, default=0.05,
                     help="serve: fraction of requests re-solved with the plain FP64 path")
     ap.add_argument("--budget-gb", type=float, default=80.0, help="batch/serve: HBM budget")
+    ap.add_argument("--body", choices=sorted(BODY_RG), default="ceres",
+                    help="solve: body of the config-1 workload (ceres is config 1 itself)")
     return ap.parse_args()
 
 
+# body of the solve-mode workload (--body): config 1 is the Ceres-like body; the others are the
+# config-3 bodies run alone, for profiling their relaunch-bound loops
+BODY = "ceres"
+BODY_RG = {"ceres": (470e3, 6.26e10), "europa": (1561e3, 3.20e12), "moon": (1737e3, 4.90e12)}
+
+
 def config_problem(N):
-    p = N.params_config(N.RUNNER_BALLISTIC, 470e3, 6.26e10, 50, SEED)
+    R, GM = BODY_RG[BODY]
+    p = N.params_config(N.RUNNER_BALLISTIC, R, GM, 50, SEED)
     ico = N.Icosphere(3)
     S = N.SurfaceInputs(ico=ico, face_T=ico.face_temperature(T_ss=235.0, T_floor=110.0))
     return p, S
@@ -627,7 +636,14 @@ def run_raytrace_mode(a):
 
 
 def main():
+    global BODY
     a = args_parse()
+    BODY = a.body
+    if BODY != "ceres":
+        R, GM = BODY_RG[BODY]
+        CONFIG["workload"] = (f"config-1 workload on a {BODY}-like body (R {R / 1e3:g} km, GM "
+                              f"{GM:g}): icosphere 1280 faces, T=max(110,235cos^0.25), dt 2 s, "
+                              f"<=20000 steps, tau 2.6e5 s, 50 exp shells to 10R x 36 x 72")
     if a.impl == "reference":
         return run_reference_arm(a)
     if a.mode == "thermal":
