@@ -219,6 +219,31 @@ def test_fast_path_is_deterministic_across_launch_shapes(ctx, N, config_surface)
         assert r["stats"] == outs[0]["stats"]
 
 
+def test_full_size_config1_shards_add_up(ctx, N, config_surface):
+    """Config 1 at its full size, 1e8 particles, where the oracle cannot follow: the grids of one
+    FAST_FP32 solve equal, cell for cell, the sums of the grids of two solves over the two halves
+    of the particle ids (fixed-point integer deposits add exactly, and every trajectory is a
+    function of its id alone), and every counter adds up."""
+    p = N.params_config(N.RUNNER_BALLISTIC)
+    n = 100_000_000
+    ctx.setup(p, config_surface)
+
+    def solve(pid_begin, count):
+        ctx.zero()
+        ctx.run(N.PATH_FAST_FP32, pid_begin, count)
+        ctx.sync()
+        return ctx.density(), ctx.horizon(), ctx.stats()
+
+    d, h, s = solve(0, n)
+    d0, h0, s0 = solve(0, n // 2)
+    d1, h1, s1 = solve(n // 2, n - n // 2)
+    np.testing.assert_array_equal(d, d0 + d1)
+    np.testing.assert_array_equal(h, h0 + h1)
+    for k in s:
+        assert s[k] == s0[k] + s1[k], k
+    assert s["n_finished"] == n and s["total_steps"] > 1000 * n
+
+
 @pytest.mark.parametrize("model", ["config", "reference"])
 def test_fast_fp32_vs_plain_fp64(ctx, N, config_surface, model):
     """Same Philox streams, FP32 compensated vs FP64: trajectories stay correlated, so the
