@@ -5,7 +5,9 @@ between particles - so a solve of N particles splits into disjoint particle-id r
 rank, with no exchange until the end. Each rank adds into its own fixed-point grids; one sum
 all-reduce of the integer density and horizon grids combines them. Particle streams are keyed by
 particle id and the grids are integer sums, so the reduced grids equal a one-GPU solve of all ids
-bit for bit (modulo-2^64 sums of the unsigned words, carried as int64).
+bit for bit (modulo-2^64 sums of the unsigned words, carried as int64). Phase 1 of a collisional
+two-phase solve reduces its per-cell speed histograms (uint64 counts) in the same call, and
+every rank fits the phase-2 CDF tables from the identical reduced counts.
 """
 from __future__ import annotations
 

@@ -19,6 +19,32 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
+def _rank_phase1(rank, world, port, out_dir):
+    """Phase 1 of the collisional two-phase solve on one rank: its id shard with per-cell speed
+    histograms, then one all-reduce of density, horizon and histograms together (the histograms
+    feed the FP64 CDF fits, which every rank then computes from the same reduced counts)."""
+    import sys
+    from datetime import timedelta
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    import torch.distributed as dist
+    from dsmc_suite_b200 import _native as N, shard
+    from oracle import oracle as O
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        p = N.params_config(N.RUNNER_BALLISTIC)
+        p.n_speed_bins = 64
+        ico = N.Icosphere(3)
+        S = N.SurfaceInputs(ico=ico, face_T=ico.face_temperature())
+        pid0, n = shard.particle_range(rank, world, N_PER_RANK)
+        r = O.run(p, S, n, pid_begin=pid0, nthreads=2, particles=False, speed_hist=True)
+        den, hor, hist = shard.allreduce_grids(dist, r["density"], r["horizon"], r["speed_hist"])
+        np.savez(os.path.join(out_dir, f"phase1_{rank}.npz"), density=den, horizon=hor, hist=hist)
+    finally:
+        dist.destroy_process_group()
+
+
 def _rank_main(rank, world, port, model, out_dir):
     import sys
     from datetime import timedelta
@@ -75,6 +101,34 @@ def test_two_rank_shards_reduce_to_the_one_process_result(N, O, tmp_path, model)
     np.testing.assert_array_equal(red["density"], np.asarray(whole["density"]).reshape(red["density"].shape))
     np.testing.assert_array_equal(red["horizon"], np.asarray(whole["horizon"]).reshape(red["horizon"].shape))
     assert red["density"].any()
+
+
+def test_two_rank_phase1_histograms_reduce_to_the_one_process_result(N, O, tmp_path):
+    """Phase 1 sharded over two gloo ranks: after one all-reduce every rank holds the density,
+    horizon and per-cell speed histograms of one process solving all ids, bit for bit, so the
+    replicated FP64 fits of phase 2 start from identical counts on every rank."""
+    import multiprocessing as mp
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_rank_phase1, args=(r, world, port, str(tmp_path)))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    p = N.params_config(N.RUNNER_BALLISTIC)
+    p.n_speed_bins = 64
+    ico = N.Icosphere(3)
+    S = N.SurfaceInputs(ico=ico, face_T=ico.face_temperature())
+    whole = O.run(p, S, world * N_PER_RANK, nthreads=2, particles=False, speed_hist=True)
+    for r in range(world):
+        red = np.load(tmp_path / f"phase1_{r}.npz")
+        np.testing.assert_array_equal(red["hist"], np.asarray(whole["speed_hist"]).reshape(red["hist"].shape))
+        np.testing.assert_array_equal(red["density"], np.asarray(whole["density"]).reshape(red["density"].shape))
+        np.testing.assert_array_equal(red["horizon"], np.asarray(whole["horizon"]).reshape(red["horizon"].shape))
+    assert red["hist"].sum() > 0
 
 
 def test_shard_ranges():
