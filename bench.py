@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the test-particle DSMC hot path on B200.
 
-Workload (one "step"): one complete solve of the config-1 ballistic problem - 1e8 H2O test
+Workload (one "step"): one complete solve of the Ceres-like ballistic problem - 1e8 H2O test
 particles per GPU on a Ceres-like body (R 470 km, GM 6.26e10), icosphere surface of 1280 faces with
 T = max(110 K, 235 K cos(z)^0.25), flux-weighted Maxwell-Boltzmann launch, Verlet dt 2 s, at most
 20,000 steps per particle, photolysis lifetime 2.6e5 s, 50 exponential shells to 10 R x 36 x 72.
@@ -53,9 +53,9 @@ def args_parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", choices=["solve", "batch", "serve", "collisional", "thermal",
                                        "raytrace"], default="solve",
-                    help="solve: one config-1 solve per step (default); batch: the 64-instance "
-                         "batch; serve: the Poisson request stream; collisional: the config-2 "
-                         "two-phase solve; thermal: the surface thermal model; raytrace: the "
+                    help="solve: one Ceres-like ballistic solve per step (default); batch: the "
+                         "64-instance batch; serve: the Poisson request stream; collisional: the "
+                         "two-phase collisional solve; thermal: the surface thermal model; raytrace: the "
                          "shadow-flux model on a synthetic cratered mesh")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--seconds", type=float, default=60.0, help="serve: arrival window [s]")
@@ -63,12 +63,13 @@ def args_parse():
                     help="serve: fraction of requests re-solved with the plain FP64 path")
     ap.add_argument("--budget-gb", type=float, default=80.0, help="batch/serve: HBM budget")
     ap.add_argument("--body", choices=sorted(BODY_RG), default="ceres",
-                    help="solve: body of the config-1 workload (ceres is config 1 itself)")
+                    help="solve: body of the ballistic workload (ceres is the default workload)")
     return ap.parse_args()
 
 
-# body of the solve-mode workload (--body): config 1 is the Ceres-like body; the others are the
-# config-3 bodies run alone, for profiling their relaunch-bound loops
+# body of the solve-mode workload (--body): the default is the Ceres-like body; the others are
+# the Europa- and Moon-like bodies of the 64-instance batch run alone, for profiling their
+# relaunch-bound loops
 BODY = "ceres"
 BODY_RG = {"ceres": (470e3, 6.26e10), "europa": (1561e3, 3.20e12), "moon": (1737e3, 4.90e12)}
 
@@ -81,7 +82,7 @@ def config_problem(N):
     return p, S
 
 
-CONFIG = {"workload": "config-1 ballistic: Ceres-like body, icosphere 1280 faces, "
+CONFIG = {"workload": "ballistic exosphere, 1e8 particles: Ceres-like body, icosphere 1280 faces, "
                       "T=max(110,235cos^0.25), dt 2 s, <=20000 steps, tau 2.6e5 s, "
                       "50 exp shells to 10R x 36 x 72",
           "solver": "FAST_FP32 resident slots, two-sum compensated push",
@@ -268,7 +269,7 @@ def plain_fp64_rate(N, device: int, problems, limit_steps: float = 4e11):
     return steps / (ms * 1e-3), k
 
 
-BATCH_CONFIG = {"workload": "config-3 batch: 64 ballistic exospheres in one queue; particles "
+BATCH_CONFIG = {"workload": "batch of 64 ballistic exospheres in one queue; particles "
                             "lognormal median 3e5 sigma_ln 1.17 clipped [1e4, 1e7]; bodies "
                             "Ceres/Europa/Moon; sub-solar T U(100,400) K, longitude uniform; "
                             "20-60 exp shells x 36 x 72; dt 2 s, <=20000 steps",
@@ -278,7 +279,7 @@ BATCH_CONFIG = {"workload": "config-3 batch: 64 ballistic exospheres in one queu
 
 
 def run_batch_mode(a):
-    """Config 3: every step submits the 64 instances and polls until all are fetched.
+    """The 64-instance batch: every step submits the instances and polls until all are fetched.
     value = particle-steps / device time of the rounds (CUDA events); e2e = the same steps /
     wall time of submit (host tables -> device) ... fetch (grids -> host)."""
     import torch
@@ -372,7 +373,7 @@ def run_batch_mode(a):
 
 
 def run_serve_mode(a):
-    """Config 4: Poisson arrivals; each request is admitted at the first poll after its arrival
+    """The served stream: Poisson arrivals; each request is admitted at the first poll after its arrival
     (or later, when the budget refuses it), and its latency runs from arrival to the poll that
     saw it complete. Throughput = particle-steps of the completed requests / wall time from the
     first arrival to the last completion."""
@@ -450,9 +451,9 @@ def run_serve_mode(a):
     line = {"metric": METRIC, "value": steps / wall, "unit": METRIC, "n_gpus": 1, "steps": 1,
             "warmup": 0, "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": f"config-4 served stream: Poisson {a.rate:g} req/s for "
-                                   f"{a.seconds:g} s, 70/30 ballistic/collisional, config-3 "
-                                   f"distributions, own seed per request",
+            "config": {"workload": f"served stream: Poisson {a.rate:g} req/s for "
+                                   f"{a.seconds:g} s, 70/30 ballistic/collisional, the 64-instance "
+                                   f"batch's distributions, own seed per request",
                        "budget_gb": a.budget_gb, "requests": len(stream),
                        "collisional": kinds.count("collisional"), "seed": SEED},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -473,7 +474,7 @@ def run_serve_mode(a):
 
 
 def run_collisional_mode(a):
-    """Config 2: phase 1 (collisionless, per-cell speed histograms) and the degree-6 FP64 fits,
+    """The two-phase collisional solve: phase 1 (collisionless, per-cell speed histograms) and the degree-6 FP64 fits,
     then each step is one phase-2 solve with hard-sphere collisions (FAST_FP32) timed with CUDA
     events; the plain FP64 path solves the same phase 2 once for the ratio and the density
     relative L2."""
@@ -491,7 +492,7 @@ def run_collisional_mode(a):
     ctx = Context(local)
     ctx.set_stream(stream.cuda_stream)
     t0 = time.perf_counter()
-    prob = W.collisional_problem(ctx, "config-2", 470e3, 6.26e10, 50, SEED, W.sun_vector(0.0),
+    prob = W.collisional_problem(ctx, "collisional-ceres", 470e3, 6.26e10, 50, SEED, W.sun_vector(0.0),
                                  235.0, n, n)
     t_phase1 = time.perf_counter() - t0
     col, p, S = prob.collision, prob.params, prob.surface
@@ -530,7 +531,7 @@ def run_collisional_mode(a):
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": "config-2 collisional two-phase: Ceres-like body, Antoine "
+            "config": {"workload": "collisional two-phase, 1e7 particles: Ceres-like body, Antoine "
                                    "sublimation-flux source on T=max(110,235cos^0.25), phase 1 "
                                    "collisionless with 64-bin speed histograms per cell, degree-6 "
                                    "FP64 CDF fits, phase 2 hard spheres d=4.6e-10 m, isotropic "
@@ -641,7 +642,7 @@ def main():
     BODY = a.body
     if BODY != "ceres":
         R, GM = BODY_RG[BODY]
-        CONFIG["workload"] = (f"config-1 workload on a {BODY}-like body (R {R / 1e3:g} km, GM "
+        CONFIG["workload"] = (f"ballistic exosphere, 1e8 particles, {BODY}-like body (R {R / 1e3:g} km, GM "
                               f"{GM:g}): icosphere 1280 faces, T=max(110,235cos^0.25), dt 2 s, "
                               f"<=20000 steps, tau 2.6e5 s, 50 exp shells to 10R x 36 x 72")
     if a.impl == "reference":

@@ -1,4 +1,4 @@
-"""Accuracy of the FP32 compensated path against the FP64 path on the config-1 workload.
+"""Accuracy of the FP32 compensated path against the FP64 path on the 1e8-particle Ceres-like ballistic workload.
 
     python -m dsmc_suite_b200.accuracy [--particles 1e8] [--trajectories 1e4] [--md out.md]
 
@@ -101,7 +101,7 @@ def markdown(res: dict, cmd: str) -> str:
     rows = "\n".join(f"| {bb:g} | {f64:.4e} | {f32:.4e} | {rd:+.2e} | {nd:+.2e} |"
                      for bb, f64, f32, rd, nd in zip(cd["b_over_R"], cd["fp64"], cd["fp32"],
                                                      cd["rel_diff"], cd["independent_run_rel_diff"]))
-    return f"""# FP32 compensated path vs FP64 path, config-1 workload
+    return f"""# FP32 compensated path vs FP64 path, 1e8-particle Ceres-like ballistic workload
 
 Command: `{cmd}`
 

@@ -33,7 +33,8 @@ __device__ __forceinline__ void accumulate(float &hi, float &lo, float b) {
 // Philox4x32-10 block of the generator's current counter, with the ten rounds kept as a loop: the
 // same words as Philox::next in a fraction of its code. The collision loop takes it in its event
 // paths (launch, start, collision), which run on single lanes: there it cuts ptxas' spill stores
-// from 416 B to 188 B and measured 7 % faster on config 2; the lean and general loops measured
+// from 416 B to 188 B and measured 7 % faster on the 1e7-particle collisional
+// phase 2; the lean and general loops measured
 // 1-3 % slower with it and keep the unrolled rounds.
 __device__ __forceinline__ void philox_next_rolled(Philox &r) {
     uint32_t c0 = r.pid, c1 = r.event, c2 = r.inst, c3 = 0u, a = r.k0, b = r.k1;
@@ -266,7 +267,7 @@ __device__ void enter_cell(const FastInst &I, Hot &h, Bounds &b, int cell) {
 // shared boundary from the registers and loads only the next one, so a typical crossing costs
 // one table load. Same cells as track_shell / track_angles. in_r, in_t, in_f are the step's own
 // inside tests per coordinate; only the coordinates that failed are walked (7 % faster on
-// config 1 than walking all three, identical cells).
+// the 1e8-particle Ceres-like workload than walking all three, identical cells).
 template <bool kNoBg>
 __device__ __forceinline__ void move_cell(const FastInst &I, Hot &h, Bounds &b, float x, float y,
                                           float r2, float zz, bool in_r, bool in_t, bool in_f) {

@@ -219,8 +219,8 @@ def test_fast_path_is_deterministic_across_launch_shapes(ctx, N, config_surface)
         assert r["stats"] == outs[0]["stats"]
 
 
-def test_full_size_config1_shards_add_up(ctx, N, config_surface):
-    """Config 1 at its full size, 1e8 particles, where the oracle cannot follow: the grids of one
+def test_full_size_ceres_workload_shards_add_up(ctx, N, config_surface):
+    """The Ceres-like ballistic workload at its full size, 1e8 particles, where the oracle cannot follow: the grids of one
     FAST_FP32 solve equal, cell for cell, the sums of the grids of two solves over the two halves
     of the particle ids (fixed-point integer deposits add exactly, and every trajectory is a
     function of its id alone), and every counter adds up."""
