@@ -45,6 +45,26 @@ def _rank_phase1(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
+def _rank_wrap(rank, world, port, out_dir):
+    """Words above 2^63 travel as negative int64: the reduced words must still be the uint64 sums
+    modulo 2^64, in the original shapes."""
+    import sys
+    from datetime import timedelta
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    import torch.distributed as dist
+    from dsmc_suite_b200 import shard
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        a = np.array([[2**63 + 5, 7], [2**64 - 1, 0]], dtype=np.uint64) + np.uint64(rank)
+        b = np.arange(5, dtype=np.uint64) * np.uint64(rank + 1)
+        ra, rb = shard.allreduce_grids(dist, a, b)
+        np.savez(os.path.join(out_dir, f"wrap_{rank}.npz"), a=ra, b=rb)
+    finally:
+        dist.destroy_process_group()
+
+
 def _rank_main(rank, world, port, model, out_dir):
     import sys
     from datetime import timedelta
@@ -129,6 +149,28 @@ def test_two_rank_phase1_histograms_reduce_to_the_one_process_result(N, O, tmp_p
         np.testing.assert_array_equal(red["density"], np.asarray(whole["density"]).reshape(red["density"].shape))
         np.testing.assert_array_equal(red["horizon"], np.asarray(whole["horizon"]).reshape(red["horizon"].shape))
     assert red["hist"].sum() > 0
+
+
+def test_two_rank_reduction_keeps_uint64_words(tmp_path):
+    import multiprocessing as mp
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_rank_wrap, args=(r, world, port, str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    a = np.array([[2**63 + 5, 7], [2**64 - 1, 0]], dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        want_a = a + a + np.uint64(1)           # modulo 2^64
+    want_b = np.arange(5, dtype=np.uint64) * np.uint64(3)
+    for r in range(world):
+        got = np.load(tmp_path / f"wrap_{r}.npz")
+        assert got["a"].dtype == np.uint64 and got["a"].shape == (2, 2)
+        np.testing.assert_array_equal(got["a"], want_a)
+        np.testing.assert_array_equal(got["b"], want_b)
 
 
 def test_shard_ranges():
