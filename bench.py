@@ -35,6 +35,7 @@ FLOPS_PER_STEP = 60   # algorithmic FP operations of one particle-step (verlet_s
                       # photolysis + deposit of the reference algorithm)
 METRIC = "particle-steps/s"
 SEED = 20261203
+E2E_CALLS = 3      # timed end-to-end calls of the solve mode (median reported)
 
 
 def args_parse():
@@ -85,8 +86,14 @@ def config_problem(N):
 CONFIG = {"workload": "ballistic exosphere, 1e8 particles: Ceres-like body, icosphere 1280 faces, "
                       "T=max(110,235cos^0.25), dt 2 s, <=20000 steps, tau 2.6e5 s, "
                       "50 exp shells to 10R x 36 x 72",
-          "solver": "FAST_FP32 resident slots, two-sum compensated push",
           "l2": "flushed before every timed step (256 MiB write)", "seed": SEED}
+SOLVER = "FAST_FP32 resident slots, two-sum compensated push"
+
+
+def workload_config(n: int, world: int) -> dict:
+    """The `config` of the solve-mode line: identical in both arms (the GPU arm and the CPU
+    reference arm describe the same workload; how each solves it goes in `solver`)."""
+    return dict(CONFIG, particles_per_gpu=n, parallelism=f"particle shards x{world}")
 
 
 class ClockSampler:
@@ -142,12 +149,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_oracle_rate(N, seconds: float, nthreads: int, n_hint: int | None = None):
+def oracle_problem():
+    """The bench workload built by the oracle's own set-up (oracle/problems.py), bit-identical to
+    config_problem's, so that the CPU legs never load the product library."""
+    from oracle import problems as OP
+    R, GM = BODY_RG[BODY]
+    p = OP.params_config(OP.RUNNER_BALLISTIC, R, GM, 50, SEED)
+    ico = OP.Icosphere(3)
+    return p, OP.SurfaceInputs(ico=ico, face_T=ico.face_temperature(T_ss=235.0, T_floor=110.0))
+
+
+def cpu_oracle_rate(seconds: float, nthreads: int, n_hint: int | None = None):
     """The oracle port (plain C, OpenMP over particles, Philox streams) on a bounded sample of
     the same workload. Returns (steps/s, particles, steps, wall seconds)."""
     from oracle import oracle as O
     O.build()
-    p, S = config_problem(N)
+    p, S = oracle_problem()
     if n_hint is None:
         t0 = time.perf_counter()
         r = O.run(p, S, 2000, nthreads=nthreads, particles=False)
@@ -180,8 +197,8 @@ def reference_binary_rate(seconds: float, nthreads: int):
     if not cli.exists():
         return None
     import tempfile
-    from dsmc_suite_b200 import _native as N
-    T = N.latlon_temperature(36, 72, T_ss=235.0, T_floor=110.0)
+    from oracle import problems as OP
+    T = OP.latlon_temperature(36, 72, T_ss=235.0, T_floor=110.0)
     with tempfile.TemporaryDirectory() as d:
         (Path(d) / "T.dat").write_text("36\n72\n" + "".join(f"{x:.17g}\n" for x in T.ravel()))
         n = 2000
@@ -203,28 +220,33 @@ def reference_binary_rate(seconds: float, nthreads: int):
 
 
 def run_reference_arm(a):
+    """The reference arm: the CPU implementation of the path (the oracle port of the reference's
+    particle loop, src/dsmc/ballistic.c:97-281, OpenMP over particles on every host core) on the
+    solve-mode workload, each step a bounded sample of it. It loads only oracle/ libraries: the
+    problem is built by oracle/problems.py. Rank 0 alone runs; other ranks exit at once."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from dsmc_suite_b200 import _native as N
     cores = os.cpu_count() or 1
     per_step = max(2.0, 90.0 / max(1, a.steps + a.warmup))
-    rate, n, steps, dt = cpu_oracle_rate(N, per_step, cores)
+    rate, n, steps, dt = cpu_oracle_rate(per_step, cores)
     for _ in range(a.warmup - 1):
-        cpu_oracle_rate(N, per_step, cores, n)
+        cpu_oracle_rate(per_step, cores, n)
     rates, secs = [], []
     for _ in range(a.steps):
-        r, _, s, d = cpu_oracle_rate(N, per_step, cores, n)
+        r, _, s, d = cpu_oracle_rate(per_step, cores, n)
         rates.append(r)
         secs.append(d)
     value = float(np.sum([r * d for r, d in zip(rates, secs)]) / np.sum(secs))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": float(np.mean(secs) * 1e3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": dict(CONFIG, solver="CPU oracle port of the reference "
-                                                "algorithm, OpenMP over particles"),
+            "data": "synthetic", "config": workload_config(int(a.particles), a.gpus),
+            "solver": "CPU oracle port of the reference algorithm, OpenMP over particles",
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
-                             "sample": f"{n} particles of the same workload per step",
+                             "sample": f"{n} particles of the same workload per step (ids from "
+                                       f"1e7); the rate is particle-steps over wall time, which "
+                                       f"per particle-step is independent of the sample size",
                              "cpu_model": cpu_model()},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -694,7 +716,7 @@ def main():
         if red is not None:
             d_ptr = red.data_ptr()
             N.check(L.dsmc_copy_grids_device(ctx.h, C_u64(d_ptr), C_u64(d_ptr + 8 * ncell)), "copy", ctx.h)
-            dist.all_reduce(red, op=dist.ReduceOp.SUM)
+            shard.allreduce_buffer(dist, red)
 
     import ctypes
     def C_u64(addr):
@@ -758,8 +780,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_ms / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-            "data": "synthetic", "config": dict(CONFIG, particles_per_gpu=n,
-                                               parallelism=f"particle shards x{world}"),
+            "data": "synthetic", "config": workload_config(n, world), "solver": SOLVER,
             "particle_steps_per_step": steps_all / a.steps, "gpu_launches": launches,
             "resident_slots": nslots, "clocks": clocks.summary(), "roofline": roofline}
 
@@ -808,10 +829,17 @@ def main():
                                       ctypes.byref(stats)), "solve_host", ctx2.h)
 
         solve_host()   # warm-up: the context's first call allocates its slots and captures graphs
-        t0 = time.perf_counter()
-        solve_host()
-        dt = time.perf_counter() - t0
-        e2e_steps = float(stats.total_steps)
+        # E2E_CALLS timed calls (each: host tables -> device, solve, grids -> host); the median
+        # call's wall time and its steps give the rate, the spread is reported beside it
+        walls, e2e_counts = [], []
+        for _ in range(E2E_CALLS):
+            t0 = time.perf_counter()
+            solve_host()
+            walls.append(time.perf_counter() - t0)
+            e2e_counts.append(float(stats.total_steps))
+        order = np.argsort(walls)
+        mid = int(order[len(order) // 2])
+        dt, e2e_steps = walls[mid], e2e_counts[mid]
         if world > 1:
             agg = torch.tensor([dt, e2e_steps], dtype=torch.float64, device="cuda")
             tmax, ssum = agg[:1].clone(), agg[1:].clone()
@@ -822,12 +850,14 @@ def main():
         line["e2e"] = {"value": e2e_steps / dt, "unit": METRIC, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": den_h.nbytes + hor_h.nbytes + ctypes.sizeof(stats),
                        "api": "dsmc_solve_host (C ABI, pinned host buffers)",
-                       "seconds": dt}
+                       "seconds": dt, "calls": len(walls),
+                       "call_seconds": [round(w, 4) for w in walls],
+                       "statistic": "median call"}
         ctx2.close()
 
     if rank == 0 and world == 1 and not a.no_cpu:
         cores = os.cpu_count() or 1
-        rate, ncpu, scpu, dcpu = cpu_oracle_rate(N, a.cpu_seconds, cores)
+        rate, ncpu, scpu, dcpu = cpu_oracle_rate(a.cpu_seconds, cores)
         line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "port",
                                 "sample": f"{ncpu} particles of the same workload, {scpu} "
                                           f"particle-steps in {dcpu:.1f} s (oracle port, OpenMP)"}
@@ -835,7 +865,7 @@ def main():
         if refbin:
             line["cpu_baseline"]["reference_binary"] = refbin
         # one thread, a quarter of the sample time: the per-core rate the OpenMP figure scales
-        r1, n1, s1, d1 = cpu_oracle_rate(N, a.cpu_seconds / 4, 1)
+        r1, n1, s1, d1 = cpu_oracle_rate(a.cpu_seconds / 4, 1)
         line["cpu_baseline"]["single_thread"] = {
             "value": r1, "unit": METRIC, "cores": 1, "kind": "port",
             "sample": f"{n1} particles, {s1} particle-steps in {d1:.1f} s"}

@@ -19,6 +19,7 @@ SCATTER_REFERENCE, SCATTER_ISOTROPIC = 0, 1
 PATH_PLAIN_FP64, PATH_FAST_FP32, PATH_FAST_FP64 = 0, 1, 2
 FATE_ALIVE, FATE_PHOTOLYSED, FATE_ESCAPED, FATE_FROZEN, FATE_STEP_CAP = range(5)
 FIXED_SCALE = 16777216.0
+VOLUME_PHYSICAL, VOLUME_REFERENCE = 0, 1
 CDF_STRIDE = 8
 CDF_MAX_DEGREE = 6
 
@@ -43,7 +44,7 @@ class Params(C.Structure):
         ("skip_first_deposit", C.c_int32), ("scatter", C.c_int32),
         ("collide_ht_max", C.c_int32), ("redraw_col_threshold", C.c_int32),
         ("seed", C.c_uint64), ("instance", C.c_uint32), ("n_speed_bins", C.c_int32),
-        ("speed_bin_width", C.c_double),
+        ("speed_bin_width", C.c_double), ("drift_tol", C.c_double),
     ]
 
     def copy(self) -> "Params":
@@ -232,6 +233,9 @@ SIGNATURES = [
                                     C.POINTER(RequestInfo)]),
     ("dsmc_server_info_get", C.c_int, [_P, C.POINTER(ServerInfo)]),
     ("dsmc_server_now", C.c_double, [_P]),
+    ("dsmc_cell_volumes", C.c_int, [C.POINTER(Params), C.c_int, _DP]),
+    ("dsmc_number_density_host", C.c_int, [C.POINTER(Params), _U64P, C.c_int64, C.c_double,
+                                           C.c_int, _DP]),
     ("dsmc_solve_host", C.c_int, [_P, C.c_int, C.POINTER(Params), C.POINTER(Surface),
                                   C.POINTER(Collision), C.c_int64, _U64P, _U64P, C.POINTER(Stats)]),
 ]
@@ -325,6 +329,23 @@ def latlon_temperature(ftd: int = 36, ffd: int = 72, sun=(1.0, 0.0, 0.0), T_ss: 
     check(lib().dsmc_latlon_temperature(ftd, ffd, ptr(s), T_ss, T_floor, ptr(T)),
           "dsmc_latlon_temperature")
     return T
+
+
+def cell_volumes(p: Params, volume_mode: int = VOLUME_PHYSICAL) -> np.ndarray:
+    """Cell volumes [hd][ftd][ffd] [m^3] (dsmc_cell_volumes)."""
+    v = np.zeros((p.hd, p.ftd, p.ffd))
+    check(lib().dsmc_cell_volumes(C.byref(p), volume_mode, ptr(v)), "dsmc_cell_volumes")
+    return v
+
+
+def number_density(p: Params, density_fx: np.ndarray, n: int, production_rate: float,
+                   volume_mode: int = VOLUME_PHYSICAL) -> np.ndarray:
+    """FP64 number density [m^-3] of a solve's fixed-point grid (dsmc_number_density_host)."""
+    fx = np.ascontiguousarray(density_fx, dtype=np.uint64)
+    out = np.zeros((p.hd, p.ftd, p.ffd))
+    check(lib().dsmc_number_density_host(C.byref(p), ptr(fx, C.c_uint64), n, production_rate,
+                                         volume_mode, ptr(out)), "dsmc_number_density_host")
+    return out
 
 
 class SurfaceInputs:

@@ -44,7 +44,7 @@ CUDA_SOURCES = {
     "dsmc_abi.cu": [],
 }
 C_SOURCES = ["host_setup.c", "host_scalar.c", "host_fileio.c", "host_runners.c", "host_thermal.c",
-             "host_raytrace.c"]
+             "host_raytrace.c", "host_density.c"]
 C_FLAGS = ["-O2", "-std=gnu11", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
            "-Wno-unused-parameter", f"-I{INC}", f"-I{CSRC}"]
 

@@ -377,7 +377,7 @@ __device__ __forceinline__ void unit_sphere_f(float zu, float pu, float o[3]) {
 }
 
 struct StatAcc {
-    unsigned steps = 0, escaped = 0, collisions = 0, bound = 0, finished = 0;
+    unsigned steps = 0, escaped = 0, collisions = 0, bound = 0, finished = 0, drift = 0;
     int inst = -1;
 };
 
@@ -387,11 +387,12 @@ __device__ void flush_stats(const FastArgs &a, StatAcc &st) {
     const unsigned full = 0xffffffffu;
     const int key = st.inst;
     const unsigned group = __match_any_sync(full, key);
-    const unsigned v[5] = {st.steps, st.escaped, st.collisions, st.bound, st.finished};
-    const int slot_of[5] = {kStatSteps, kStatEscaped, kStatCollisions, kStatBound, kStatFinished};
+    const unsigned v[6] = {st.steps, st.escaped, st.collisions, st.bound, st.finished, st.drift};
+    const int slot_of[6] = {kStatSteps, kStatEscaped, kStatCollisions, kStatBound, kStatFinished,
+                            kStatDrift};
     const bool leader = (threadIdx.x & 31) == (__ffs(group) - 1);
 #pragma unroll
-    for (int k = 0; k < 5; k++) {
+    for (int k = 0; k < 6; k++) {
         const unsigned sum = __reduce_add_sync(group, v[k]);
         if (leader && key >= 0 && sum)
             atomicAdd(&a.inst[key].t.stats[slot_of[k]], static_cast<unsigned long long>(sum));
@@ -408,6 +409,7 @@ __device__ void flush_stats_lane(const FastArgs &a, StatAcc &st) {
         if (st.escaped) atomicAdd(dst + kStatEscaped, static_cast<unsigned long long>(st.escaped));
         if (st.collisions) atomicAdd(dst + kStatCollisions, static_cast<unsigned long long>(st.collisions));
         if (st.bound) atomicAdd(dst + kStatBound, static_cast<unsigned long long>(st.bound));
+        if (st.drift) atomicAdd(dst + kStatDrift, static_cast<unsigned long long>(st.drift));
         if (st.finished) {
             atomicAdd(dst + kStatFinished, static_cast<unsigned long long>(st.finished));
             atomicAdd(&a.ctr->finished, static_cast<unsigned long long>(st.finished));
@@ -435,6 +437,34 @@ __device__ __forceinline__ void angles_of(const Hot &h, float &thi, float &fi) {
     double f = atan2(s[0], s[1]);
     if (f < 0) f += 2.0 * kPi;
     fi = static_cast<float>(f);
+}
+
+// Orbital energy per unit mass |v|^2 / 2 - GM / |s| of the current state in FP64, for the
+// per-hop energy-drift guard: 1 / |s| from the FP32 reciprocal square root and one Newton step in
+// FP64 (relative error ~1e-14), so the event path takes no FP64 square root or division.
+__device__ __forceinline__ double orbital_energy(const FastInst &I, const Hot &h) {
+    double s[3], v[3];
+    get_pos(h, s);
+    get_vel(h, v);
+    const double r2 = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+    double ir = rsqrtf(static_cast<float>(r2));
+    ir = ir * (1.5 - 0.5 * r2 * ir * ir);
+    return 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) - I.p.GM * ir;
+}
+
+// The hop's energy baseline: taken at every launch and after every collision.
+__device__ __forceinline__ void drift_start(const FastArgs &a, long long i, const FastInst &I,
+                                            const Hot &h) {
+    if (I.drift_abs > 0.0) a.s.e0[i] = static_cast<float>(orbital_energy(I, h));
+}
+
+// The hop ended (landing, escape radius, hop or life cap): counts it when the energy moved by
+// more than the guard's bound since the baseline.
+__device__ __forceinline__ void drift_check(const FastArgs &a, long long i, const FastInst &I,
+                                            const Hot &h, StatAcc &st) {
+    if (I.drift_abs > 0.0 &&
+        fabs(orbital_energy(I, h) - static_cast<double>(a.s.e0[i])) > I.drift_abs)
+        st.drift++;
 }
 
 __device__ __forceinline__ void horizon_add(const FastInst &I, int td, int fd, float W) {
@@ -517,6 +547,7 @@ __device__ bool launch(const FastArgs &a, long long i, const FastInst &I, Hot &h
     h.oa[1] = g * sy;
     h.oa[2] = g * sz;
     h.hop = 0;
+    drift_start(a, i, I, h);
     return true;
 }
 
@@ -771,6 +802,7 @@ __device__ void collide(const FastArgs &a, long long i, const FastInst &I, Hot &
     if (col_p >= 0.0) h.pthr = -log1pf(-static_cast<float>(col_p));
     set_vel(h, v);
     h.pcol = 0.0f;
+    drift_start(a, i, I, h);
 }
 
 // Next work index of the device queue: one atomic per group of lanes asking together.
@@ -1047,6 +1079,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
             if (!event && h.steps >= life_cap) event = 3;
         }
         if (event) {
+            drift_check(a, i, *I, h, st);
             int fate = 0;
             if (event == 2) {
                 fate = DSMC_FATE_ESCAPED;
@@ -1274,36 +1307,9 @@ cudaError_t FastEngine::ensure_slots(int num_sms) {
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (slot_mem_) { cudaFree(slot_mem_); slot_mem_ = nullptr; }
     const long long S = want;
-    // 4-byte fields: inst pid evt (3) + 15 vector floats + w0 nday steps hop cell run_cell
-    // hist_key hist_cnt pcol pthr ncol rest wcur face (14) = 32 words; plus run_w (8-byte slot).
-    const size_t bytes = static_cast<size_t>(S) * (32 * 4 + 8) + 256;
-    cudaError_t e = cudaMalloc(&slot_mem_, bytes);
+    cudaError_t e = cudaMalloc(&slot_mem_, fast_slot_bytes(S));
     if (e != cudaSuccess) return e;
-    char *b = static_cast<char *>(slot_mem_);
-    auto take = [&](size_t each) { char *p = b; b += static_cast<size_t>(S) * each; return p; };
-    slots_.run_w = reinterpret_cast<float *>(take(8));
-    slots_.inst = reinterpret_cast<int *>(take(4));
-    slots_.pid = reinterpret_cast<unsigned *>(take(4));
-    slots_.evt = reinterpret_cast<unsigned *>(take(4));
-    slots_.sh = reinterpret_cast<float *>(take(12));
-    slots_.sl = reinterpret_cast<float *>(take(12));
-    slots_.vh = reinterpret_cast<float *>(take(12));
-    slots_.vl = reinterpret_cast<float *>(take(12));
-    slots_.oa = reinterpret_cast<float *>(take(12));
-    slots_.w0 = reinterpret_cast<float *>(take(4));
-    slots_.nday = reinterpret_cast<int *>(take(4));
-    slots_.steps = reinterpret_cast<int *>(take(4));
-    slots_.hop = reinterpret_cast<int *>(take(4));
-    slots_.cell = reinterpret_cast<int *>(take(4));
-    slots_.run_cell = reinterpret_cast<int *>(take(4));
-    slots_.hist_key = reinterpret_cast<int *>(take(4));
-    slots_.hist_cnt = reinterpret_cast<int *>(take(4));
-    slots_.pcol = reinterpret_cast<float *>(take(4));
-    slots_.pthr = reinterpret_cast<float *>(take(4));
-    slots_.ncol = reinterpret_cast<int *>(take(4));
-    slots_.rest = reinterpret_cast<float *>(take(4));
-    slots_.wcur = reinterpret_cast<float *>(take(4));
-    slots_.face = reinterpret_cast<int *>(take(4));
+    slots_ = carve_slots(slot_mem_, S);
     nslots_ = S;
     if (!d_ctr_) {
         if ((e = cudaMalloc(&d_ctr_, sizeof(FastCounters))) != cudaSuccess) return e;
@@ -1372,6 +1378,7 @@ cudaError_t FastEngine::upload_instances(const std::vector<dsmc_params> &ps,
         I.n = counts[k];
         I.pid_begin = pid_begins[k];
         I.c_day = static_cast<float>(p.dt_step / p.lifetime / std::log(2.0));
+        I.drift_abs = p.drift_tol > 0.0 ? p.drift_tol * p.GM / p.Radii : 0.0;
         I.r_land2 = static_cast<float>(p.Radii * p.Radii);
         I.r_esc2 = static_cast<float>(p.max_height * p.max_height);
         // device addresses filled below
@@ -1667,7 +1674,38 @@ size_t FastEngine::serve_fixed_bytes(int max_instances) const {
 }
 
 size_t fast_slot_bytes(long long nslots) {
-    return static_cast<size_t>(nslots) * (32 * 4 + 8) + 256;
+    return static_cast<size_t>(nslots) * kSlotBytesPerSlot + 256;
+}
+
+Slots carve_slots(void *mem, long long S) {
+    char *b = static_cast<char *>(mem);
+    auto take = [&](size_t each) { char *q = b; b += static_cast<size_t>(S) * each; return q; };
+    Slots s{};
+    s.run_w = reinterpret_cast<float *>(take(8));
+    s.inst = reinterpret_cast<int *>(take(4));
+    s.pid = reinterpret_cast<unsigned *>(take(4));
+    s.evt = reinterpret_cast<unsigned *>(take(4));
+    s.sh = reinterpret_cast<float *>(take(12));
+    s.sl = reinterpret_cast<float *>(take(12));
+    s.vh = reinterpret_cast<float *>(take(12));
+    s.vl = reinterpret_cast<float *>(take(12));
+    s.oa = reinterpret_cast<float *>(take(12));
+    s.w0 = reinterpret_cast<float *>(take(4));
+    s.nday = reinterpret_cast<int *>(take(4));
+    s.steps = reinterpret_cast<int *>(take(4));
+    s.hop = reinterpret_cast<int *>(take(4));
+    s.cell = reinterpret_cast<int *>(take(4));
+    s.run_cell = reinterpret_cast<int *>(take(4));
+    s.hist_key = reinterpret_cast<int *>(take(4));
+    s.hist_cnt = reinterpret_cast<int *>(take(4));
+    s.pcol = reinterpret_cast<float *>(take(4));
+    s.pthr = reinterpret_cast<float *>(take(4));
+    s.ncol = reinterpret_cast<int *>(take(4));
+    s.rest = reinterpret_cast<float *>(take(4));
+    s.wcur = reinterpret_cast<float *>(take(4));
+    s.face = reinterpret_cast<int *>(take(4));
+    s.e0 = reinterpret_cast<float *>(take(4));
+    return s;
 }
 
 size_t fast_inst_bytes() { return sizeof(FastInst); }
@@ -1712,6 +1750,7 @@ cudaError_t fast_fill_instance(const dsmc_params &p, const DevTables &t, long lo
     I.n = n;
     I.pid_begin = pid_begin;
     I.c_day = static_cast<float>(p.dt_step / p.lifetime / std::log(2.0));
+    I.drift_abs = p.drift_tol > 0.0 ? p.drift_tol * p.GM / p.Radii : 0.0;
     I.r_land2 = static_cast<float>(p.Radii * p.Radii);
     I.r_esc2 = static_cast<float>(p.max_height * p.max_height);
     return cudaSuccess;
@@ -1719,37 +1758,13 @@ cudaError_t fast_fill_instance(const dsmc_params &p, const DevTables &t, long lo
 
 cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long nslots, void *d_ctr,
                                 long long total, int steps_per_launch, int block,
-                                cudaStream_t stream, long long *launches) {
+                                long long stall_launches, cudaStream_t stream,
+                                long long *launches) {
     *launches = 0;
     if (total <= 0) return cudaSuccess;
     if (nslots % block) return cudaErrorInvalidValue;
     const long long S = nslots;
-    char *b = static_cast<char *>(slot_mem);
-    auto take = [&](size_t each) { char *q = b; b += static_cast<size_t>(S) * each; return q; };
-    Slots s{};
-    s.run_w = reinterpret_cast<float *>(take(8));
-    s.inst = reinterpret_cast<int *>(take(4));
-    s.pid = reinterpret_cast<unsigned *>(take(4));
-    s.evt = reinterpret_cast<unsigned *>(take(4));
-    s.sh = reinterpret_cast<float *>(take(12));
-    s.sl = reinterpret_cast<float *>(take(12));
-    s.vh = reinterpret_cast<float *>(take(12));
-    s.vl = reinterpret_cast<float *>(take(12));
-    s.oa = reinterpret_cast<float *>(take(12));
-    s.w0 = reinterpret_cast<float *>(take(4));
-    s.nday = reinterpret_cast<int *>(take(4));
-    s.steps = reinterpret_cast<int *>(take(4));
-    s.hop = reinterpret_cast<int *>(take(4));
-    s.cell = reinterpret_cast<int *>(take(4));
-    s.run_cell = reinterpret_cast<int *>(take(4));
-    s.hist_key = reinterpret_cast<int *>(take(4));
-    s.hist_cnt = reinterpret_cast<int *>(take(4));
-    s.pcol = reinterpret_cast<float *>(take(4));
-    s.pthr = reinterpret_cast<float *>(take(4));
-    s.ncol = reinterpret_cast<int *>(take(4));
-    s.rest = reinterpret_cast<float *>(take(4));
-    s.wcur = reinterpret_cast<float *>(take(4));
-    s.face = reinterpret_cast<int *>(take(4));
+    const Slots s = carve_slots(slot_mem, S);
     cudaError_t e;
     FastCounters host{};
     host.total = static_cast<unsigned long long>(total);
@@ -1768,7 +1783,7 @@ cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long ns
     unsigned long long last = 0;
     long long stalled = 0;
     for (;;) {
-        if (stalled > 4096) return cudaErrorLaunchTimeout;
+        if (stalled > stall_launches) return cudaErrorLaunchTimeout;
         fast_kernel<256, 2, 0><<<grid, block, 0, stream>>>(a);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         *launches += 1;

@@ -24,6 +24,7 @@ struct FastInst {
     long long pid_begin;     // particle id of the first particle
     float c_day;             // h / lifetime / ln 2 (W = W0 * 2^(-c_day * n_day))
     float r_land2, r_esc2;   // Radii^2, max_height^2
+    double drift_abs;        // drift_tol * GM / Radii: the energy-drift guard's bound (0 = off)
     const float4 *face_f;    // FP32 icosphere tables (config model), or nullptr: FP64 descent
 };
 
@@ -53,7 +54,15 @@ struct Slots {
     float *rest;             // freeze waiting time (reference model)
     float *wcur;             // running weight (the hot loop's W between launches)
     int *face;               // icosphere face of the last launch point (config model), -1 = none
+    float *e0;               // orbital energy at the hop's launch or last collision (drift guard)
 };
+
+// Bytes of one slot in the structure-of-arrays block: run_w (8-byte slot) plus 33 four-byte
+// fields (inst pid evt, 15 vector floats, w0 nday steps hop cell run_cell hist_key hist_cnt pcol
+// pthr ncol rest wcur face e0). carve_slots lays the arrays out in that order over slot memory of
+// fast_slot_bytes(nslots) bytes.
+constexpr size_t kSlotBytesPerSlot = 33 * 4 + 8;
+Slots carve_slots(void *mem, long long nslots);
 
 // Device-side queue state. `total` and `ninst` live here rather than in the kernel arguments so
 // that the host can append instances between launches of an already captured graph.
@@ -68,7 +77,9 @@ struct FastCounters {
 // bytes of the slot arrays for nslots slots, of one instance descriptor and of the counters;
 // fast_fill_instance builds one descriptor and its boundary tables in host memory (tab_host,
 // tab_floats entries; d_tab is where the caller will copy them); fast_drain_external runs the
-// launch loop without graphs on caller memory until the queue of `total` particles is empty.
+// launch loop without graphs on caller memory until the queue of `total` particles is empty, and
+// gives up (cudaErrorLaunchTimeout) after stall_launches launches in a row in which no particle
+// finished.
 size_t fast_slot_bytes(long long nslots);
 size_t fast_inst_bytes();
 size_t fast_counter_bytes();
@@ -77,7 +88,8 @@ cudaError_t fast_fill_instance(const dsmc_params &p, const DevTables &t, long lo
                                float *tab_host);
 cudaError_t fast_drain_external(const void *d_inst, void *slot_mem, long long nslots, void *d_ctr,
                                 long long total, int steps_per_launch, int block,
-                                cudaStream_t stream, long long *launches);
+                                long long stall_launches, cudaStream_t stream,
+                                long long *launches);
 
 class FastEngine {
 public:

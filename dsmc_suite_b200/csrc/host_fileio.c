@@ -51,6 +51,18 @@ int write_density_dat(const char *filename, const double *den, int ftd, int ffd,
     return fclose(fp) == 0 ? 0 : -1;
 }
 
+/* Addition (no reference counterpart): number density [m^-3], header ftd, ffd, hd as the
+ * density file, then [hd][ftd][ffd] values in %.9e (the density file's %9.6f is fixed point). */
+int write_ndensity_dat(const char *filename, const double *nden, int ftd, int ffd, int hd)
+{
+    FILE *fp = open_or_report(filename, "w");
+    if (!fp) return -1;
+    fprintf(fp, "%d\n%d\n%d\n", ftd, ffd, hd);
+    const long n = (long)hd * ftd * ffd;
+    for (long i = 0; i < n; i++) fprintf(fp, "%.9e\n", nden[i]);
+    return fclose(fp) == 0 ? 0 : -1;
+}
+
 /* Reference: fileio.c:47-62. Header ftd, ffd, then [ftd][ffd]. */
 double *read_temperature_dat(const char *filename, int *ftd, int *ffd)
 {

@@ -79,6 +79,17 @@ static void write_grids(const char *prefix, const uint64_t *den, const uint64_t 
         write_horizon_dat(fname, hh, p->ftd, p->ffd);
         snprintf(fname, sizeof fname, "%s_ttime.dat", prefix);
         write_ttime_dat(fname, ttime, nrows, totaln);
+        const char *rate = getenv("DSMC_NDENSITY_RATE");
+        if (rate && *rate && totaln > 0) {
+            /* FP64 number density [m^-3] per cell, physical cell volumes */
+            double *nd = malloc((size_t)ncell * sizeof(double));
+            snprintf(fname, sizeof fname, "%s_ndensity.dat", prefix);
+            if (!nd || dsmc_number_density_host(p, den, totaln, strtod(rate, NULL),
+                                                DSMC_VOLUME_PHYSICAL, nd) != DSMC_OK ||
+                write_ndensity_dat(fname, nd, p->ftd, p->ffd, p->hd))
+                fprintf(stderr, "cannot write %s\n", fname);
+            free(nd);
+        }
         if (env_int("DSMC_SIDECAR", 0)) {
             snprintf(fname, sizeof fname, "%s_grids.bin", prefix);
             if (write_grids_bin(fname, den, hor, ttime, p->ftd, p->ffd, p->hd, nrows, totaln,

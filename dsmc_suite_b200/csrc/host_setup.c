@@ -37,6 +37,7 @@ static void common_reference(dsmc_params *p, int ftd, int ffd)
     p->w_min = 0.01;
     p->hop_step_cap = 10000000;
     p->life_step_cap = 0;
+    p->drift_tol = 1e-2;
     p->scatter = DSMC_SCATTER_REFERENCE;
     p->seed = 20261203u;
 }
@@ -116,6 +117,7 @@ int dsmc_params_config(dsmc_params *p, int runner, double Radii, double GM, int 
     p->seed = seed;
     p->n_speed_bins = 0;
     p->speed_bin_width = 25.0;
+    p->drift_tol = 1e-2;
     return DSMC_OK;
 }
 

@@ -70,8 +70,14 @@ __device__ __forceinline__ void unit_sphere(double zu, double pu, double o[3]) {
 }
 
 struct Acc {
-    unsigned long long steps = 0, escaped = 0, collisions = 0, bound = 0, finished = 0;
+    unsigned long long steps = 0, escaped = 0, collisions = 0, bound = 0, finished = 0, drift = 0;
 };
+
+// Orbital energy per unit mass |v|^2 / 2 - GM / |s| of the per-hop energy-drift guard.
+__device__ __forceinline__ double orbital_energy(const dsmc_params &p, const double s[3],
+                                                 const double v[3]) {
+    return 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) - p.GM / len3(s);
+}
 
 // Velocity-record replay modes (see launch_plain_record): kCount counts the deposited visits of
 // each particle per (td, ht) bucket into the particle's own row; kRecord turns those rows into
@@ -94,6 +100,9 @@ __device__ void particle_life(const dsmc_params &p, const DevTables &t, long lon
     long long steps = 0;
     double real_col_p = 0.0, col_p = 0.0, time = 0.0, W = 1.0, flight_time = 0.0,
            rest_time = 0.0, thi, fi, local_T, s[3], v[3] = {0.0, 0.0, 0.0};
+    // energy-drift guard: E at the hop's launch (or last collision) against E where it ends
+    const double drift_abs = p.drift_tol * p.GM / p.Radii;
+    double E_start = 0.0;
 
     rng.next();
     if (ref) {
@@ -220,6 +229,7 @@ __device__ void particle_life(const dsmc_params &p, const DevTables &t, long lon
         double Ri = len3(s);
         double oa[3];
         for (int k = 0; k < 3; k++) oa[k] = p.GM * s[k] / (Ri * Ri * Ri);
+        E_start = orbital_energy(p, s, v);
 
         for (long long ii = 0; ii < p.hop_step_cap; ii++) {
             flight_time += h;
@@ -306,6 +316,7 @@ __device__ void particle_life(const dsmc_params &p, const DevTables &t, long lon
                             for (int k = 0; k < 3; k++) v[k] = vcm[k] + 0.5 * gl * om[k];
                         }
                         collided = true;
+                        E_start = orbital_energy(p, s, v);
                     }
                 }
                 if (kMode != kSolve) {
@@ -338,6 +349,8 @@ __device__ void particle_life(const dsmc_params &p, const DevTables &t, long lon
                 break;
             }
         }
+        // the hop ended (landing, escape radius, hop or life cap)
+        if (p.drift_tol > 0.0 && fabs(orbital_energy(p, s, v) - E_start) > drift_abs) acc.drift++;
         if (fate != DSMC_FATE_ALIVE) break;
 
         // Landing, ballistic.c:239-264.
@@ -394,6 +407,7 @@ __global__ void __launch_bounds__(128) plain_fp64_kernel(const dsmc_params p, co
         warp_add_stat(&t.stats[kStatCollisions], acc.collisions);
         warp_add_stat(&t.stats[kStatBound], acc.bound);
         warp_add_stat(&t.stats[kStatFinished], acc.finished);
+        warp_add_stat(&t.stats[kStatDrift], acc.drift);
     }
 }
 

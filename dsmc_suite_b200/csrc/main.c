@@ -53,7 +53,10 @@ static void print_usage(const char *prog)
     printf("  -v <v_record_file> Velocity record file (for dsmc-adv)\n");
     printf("  -o <output_prefix> Output file prefix (default: output)\n");
     printf("  --bin              Also write <prefix>_grids.bin (exact grids, FP64 rows)\n");
-    printf("Environment: DSMC_DEVICE, DSMC_PATH (plain|fast32), DSMC_SEED, DSMC_SIDECAR\n");
+    printf("  --ndensity <Q>     Also write <prefix>_ndensity.dat: FP64 number density [m^-3]\n");
+    printf("                     for a production rate of Q molecules/s\n");
+    printf("Environment: DSMC_DEVICE, DSMC_PATH (plain|fast32|fast64), DSMC_SEED, DSMC_SIDECAR,\n");
+    printf("             DSMC_NDENSITY_RATE\n");
 }
 
 int main(int argc, char *argv[])
@@ -82,6 +85,7 @@ int main(int argc, char *argv[])
         else if (!strcmp(argv[i], "--tt") && more) tt = atoi(argv[++i]);
         else if (!strcmp(argv[i], "--nmonte") && more) nmonte = atoi(argv[++i]);
         else if (!strcmp(argv[i], "--bin")) setenv("DSMC_SIDECAR", "1", 1);
+        else if (!strcmp(argv[i], "--ndensity") && more) setenv("DSMC_NDENSITY_RATE", argv[++i], 1);
     }
     if (!strcmp(command, "dsmc")) {
         run_ballistic(totaln, temp_file, output_prefix, nthreads);

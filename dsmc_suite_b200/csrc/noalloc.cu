@@ -31,10 +31,11 @@ constexpr size_t round_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign;
 // Stated maximum sizes of the no-allocation path.
 constexpr long long kSlots = 32768;        // resident particle slots (threads)
 constexpr int kBlock = 128;                // threads per block: 256 blocks of 128
+constexpr int kStepsPerLaunch = 8192;      // Verlet steps per slot per launch (the engine's)
 constexpr size_t kTabFloats = 4096;        // (hd+1) + (ftd+1) + 2 (ffd+1) + 1 floats at most
 
 constexpr size_t kSlotOff = 0;
-constexpr size_t kSlotBytes = round_up(static_cast<size_t>(kSlots) * (32 * 4 + 8) + 256);
+constexpr size_t kSlotBytes = round_up(static_cast<size_t>(kSlots) * dsmc::kSlotBytesPerSlot + 256);
 constexpr size_t kInstOff = kSlotOff + kSlotBytes;
 constexpr size_t kInstBytes = round_up(sizeof(dsmc::FastInst));
 constexpr size_t kTabOff = kInstOff + kInstBytes;
@@ -84,8 +85,11 @@ extern "C" int dsmc_solve_fast_noalloc(const dsmc_params *p, const dsmc_surface 
                                        uint64_t *horizon, uint64_t *stats, void *stream_ptr) {
     if (!p || !surf || !density || !horizon || !stats)
         return fail(DSMC_ERR_INVALID, "params, surface, density, horizon and stats are required");
-    if (n < 0 || pid_begin < 0 || pid_begin + n > (int64_t(1) << 32))
+    constexpr int64_t kIds = int64_t(1) << 32;
+    if (n < 0 || pid_begin < 0 || n > kIds || pid_begin > kIds - n)
         return fail(DSMC_ERR_INVALID, "particle ids must lie in [0, 2^32)");
+    if (p->model != DSMC_MODEL_REFERENCE && p->model != DSMC_MODEL_CONFIG)
+        return fail(DSMC_ERR_INVALID, "unknown physics model");
     if (p->runner != DSMC_RUNNER_BALLISTIC)
         return fail(DSMC_ERR_INVALID, "the no-allocation path solves the ballistic runner only");
     if (p->ftd < 1 || p->ffd < 2 || p->hd < 1 || p->ftd > 255 || p->ffd > 255 ||
@@ -161,9 +165,17 @@ extern "C" int dsmc_solve_fast_noalloc(const dsmc_params *p, const dsmc_surface 
     // the statistics start at zero; density and horizon are added into
     if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, dsmc::kStatCount * sizeof(uint64_t), stream);
     if (e != cudaSuccess) return fail_cuda("scratch set-up", e);
+    // The drain gives up when no particle has finished for stall_launches launches in a row.
+    // A legal solve can go that long only while its last particles fly: at most one hop of
+    // hop_step_cap steps ends without a finish, and a life ends by its cap; the limit allows
+    // twice the longest hop plus the life cap, and never fewer than 2^28 steps.
+    const double hop = static_cast<double>(p->hop_step_cap);
+    const double life = p->life_step_cap > 0 ? static_cast<double>(p->life_step_cap) : 0.0;
+    const double quiet_steps = hop * 2.0 + life > 268435456.0 ? hop * 2.0 + life : 268435456.0;
+    const long long stall_launches = static_cast<long long>(quiet_steps / kStepsPerLaunch) + 1;
     long long launches = 0;
     e = dsmc::fast_drain_external(base + kInstOff, base + kSlotOff, kSlots, base + kCtrOff, n,
-                                  2048, kBlock, stream, &launches);
+                                  kStepsPerLaunch, kBlock, stall_launches, stream, &launches);
     if (e != cudaSuccess) return fail_cuda("fast solve", e);
     return DSMC_OK;
 }

@@ -30,15 +30,27 @@ def split_range(rank: int, world: int, n_total: int) -> tuple[int, int]:
     return begin, base + (1 if rank < extra else 0)
 
 
+def allreduce_buffer(dist, buf) -> None:
+    """The one collective of a sharded solve: an in-place sum all-reduce of an int64 torch tensor
+    that holds a rank's fixed-point grids back to back (density, horizon and, in phase 1 of a
+    collisional solve, the speed histograms). The unsigned 64-bit words travel as int64, whose
+    two's-complement sums are the modulo-2^64 sums of the words. `buf` lives on the rank's GPU
+    for NCCL (bench.py fills it with dsmc_copy_grids_device) or on the CPU for gloo."""
+    import torch
+    if buf.dtype != torch.int64 or not buf.is_contiguous():
+        raise ValueError("the grid buffer must be a contiguous int64 tensor")
+    dist.all_reduce(buf, op=dist.ReduceOp.SUM)
+
+
 def allreduce_grids(dist, *grids: np.ndarray, device=None) -> list[np.ndarray]:
-    """Sum uint64 grids over the process group (one collective for all of them). `device` is
+    """Sum uint64 host grids over the process group with one allreduce_buffer call. `device` is
     the torch device of the communication buffer ("cuda" for NCCL, None/CPU for gloo)."""
     import torch
     flat = np.concatenate([g.ravel().view(np.int64) for g in grids])
     t = torch.from_numpy(flat.copy())
     if device is not None:
         t = t.to(device)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    allreduce_buffer(dist, t)
     out = t.cpu().numpy().view(np.uint64)
     res, k = [], 0
     for g in grids:

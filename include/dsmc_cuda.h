@@ -195,6 +195,21 @@ int dsmc_solve_host(dsmc_ctx *ctx, int path, const dsmc_params *p, const dsmc_su
                     uint64_t *horizon_fx, dsmc_stats *stats);
 
 /* ---------------------------------------------------------------------------------------- */
+/* FP64 number density (host, no device needed).                                             */
+/* The reference writes raw weight sums (src/dsmc/ballistic.c:235-236) and never divides by the */
+/* volumes that src/common/grid.c:41-84 computes. These turn the fixed-point grid of a solve    */
+/* into molecules per m^3: n test particles stand for production_rate molecules/s, one         */
+/* deposited weight-step is dt_step seconds of residence, so                                  */
+/*     nden[c] = density_fx[c] / 2^24 * production_rate / n * dt_step / volume[c]             */
+/* in FP64. DSMC_VOLUME_PHYSICAL: spherical-shell cells (r_o^3 - r^3) / 3 * dphi *            */
+/* |sin b_o - sin b|; DSMC_VOLUME_REFERENCE: the reference's grid_compute_volume_uniform /     */
+/* _exp (grid.c:41-84, which adds the two cubes). Arrays [hd][ftd][ffd].                      */
+enum dsmc_volume { DSMC_VOLUME_PHYSICAL = 0, DSMC_VOLUME_REFERENCE = 1 };
+int dsmc_cell_volumes(const dsmc_params *p, int volume_mode, double *volume);
+int dsmc_number_density_host(const dsmc_params *p, const uint64_t *density_fx, int64_t n,
+                             double production_rate, int volume_mode, double *nden);
+
+/* ---------------------------------------------------------------------------------------- */
 /* FAST_FP32 solve without any device allocation.                                            */
 /* (This entry point has no counterpart in the reference.)                                   */
 /*                                                                                           */
@@ -216,10 +231,10 @@ int dsmc_solve_host(dsmc_ctx *ctx, int path, const dsmc_params *p, const dsmc_su
 /* exits. Larger grids are rejected with DSMC_ERR_INVALID. The first call on a device looks  */
 /* up the array's device address (cudaGetSymbolAddress); make that first call before any     */
 /* stream capture. Every call shares the array and it keeps the last call's contents (the   */
-/* call resets what must start at zero): calls from this process are serialised, but calls  */
-/* whose GPU work overlaps - e.g. one issued while a previous one is still being replayed    */
-/* from a captured graph - race on the array. dsmc_noalloc_last_error() describes the last   */
-/* failure. */
+/* call resets what must start at zero). Calls whose GPU work overlapped would race on the  */
+/* array; the library prevents that within a process: calls are serialised by a lock and    */
+/* each returns only after its GPU work has finished (the host reads the work-queue counters */
+/* after every launch). dsmc_noalloc_last_error() describes the last failure. */
 int dsmc_solve_fast_noalloc(const dsmc_params *p, const dsmc_surface *surf, int64_t pid_begin,
                             int64_t n, uint64_t *density, uint64_t *horizon, uint64_t *stats,
                             void *stream);

@@ -79,6 +79,13 @@ typedef struct dsmc_params {
     uint32_t instance;      /* Philox counter word, distinguishes instances of one batch */
     int32_t n_speed_bins;   /* config phase-1 speed histogram bins per cell (0 = off) */
     double speed_bin_width; /* [m/s] */
+    /* Per-hop energy-drift guard (FP64). E = |v|^2 / 2 - GM / |s| is taken at every launch and
+     * after every collision, and again where the hop ends (landing, escape radius, hop or life
+     * cap); a hop whose |E_end - E_start| exceeds drift_tol * GM / Radii is counted in
+     * dsmc_stats.n_drift_flagged. The trajectory itself is not changed. 0 turns the guard off.
+     * The reference's integrator (src/common/integrator.c:4-55: first-order velocity update)
+     * drifts by about 1e-3 GM / R over a typical hop at its time steps; the presets use 1e-2. */
+    double drift_tol;
 } dsmc_params;
 
 /* Surface description. The reference model reads a latitude-longitude temperature map

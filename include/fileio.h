@@ -28,4 +28,8 @@ int write_grids_bin(const char *filename, const uint64_t *den, const uint64_t *h
                     const double *ttime, int ftd, int ffd, int hd, int nrows, int totaln,
                     double fixed_scale);
 
+/* Addition (no reference counterpart): <prefix>_ndensity.dat, the FP64 number density [m^-3]
+ * of dsmc_number_density_host: header ftd, ffd, hd, then [hd][ftd][ffd] values in %.9e. */
+int write_ndensity_dat(const char *filename, const double *nden, int ftd, int ffd, int hd);
+
 #endif /* FILEIO_H */

@@ -441,6 +441,12 @@ static int pick_face(const dsmc_surface *surf, double u)
     return lo;
 }
 
+/* Orbital energy per unit mass |v|^2 / 2 - GM / |s| of the drift guard. */
+static double orbital_energy(const dsmc_params *p, const double s[3], const double v[3])
+{
+    return 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) - p->GM / len3(s);
+}
+
 static void run_particle(or_ctx *c, int64_t pid, or_rng *r)
 {
     const dsmc_params *p = c->p;
@@ -462,6 +468,9 @@ static void run_particle(or_ctx *c, int64_t pid, or_rng *r)
     double thi, fi, s[3], v[3] = {0.0, 0.0, 0.0};
     double local_T = 0.0;
     int td, fd;
+    /* energy-drift guard: E at the hop's launch (or last collision) against E where it ends */
+    const double drift_abs = p->drift_tol * p->GM / p->Radii;
+    double E_start = 0.0;
 
     r->pid = (uint32_t)pid;
     r->event = 0;
@@ -562,6 +571,7 @@ static void run_particle(or_ctx *c, int64_t pid, or_rng *r)
         double Ri = len3(s);
         double oa[3];
         for (int k = 0; k < 3; k++) oa[k] = p->GM * s[k] / (Ri * Ri * Ri);
+        E_start = orbital_energy(p, s, v);
 
         for (int64_t ii = 0; ii < p->hop_step_cap; ii++) {
             flight_time += h;
@@ -648,6 +658,7 @@ static void run_particle(or_ctx *c, int64_t pid, or_rng *r)
                             for (int k = 0; k < 3; k++) v[k] = vcm[k] + 0.5 * gl * om[k];
                         }
                         collided = 1;
+                        E_start = orbital_energy(p, s, v);
                     }
                 }
                 if (!collided) {
@@ -666,6 +677,9 @@ static void run_particle(or_ctx *c, int64_t pid, or_rng *r)
                 break;
             }
         }
+        /* the hop ended (landing, escape radius, hop or life cap) */
+        if (p->drift_tol > 0.0 && fabs(orbital_energy(p, s, v) - E_start) > drift_abs)
+            add_i64(&out->n_drift_flagged, 1, c->serial);
         if (fate != DSMC_FATE_ALIVE) break;
 
         /* landing (or a hop that ran out of steps): ballistic.c:239-264 */

@@ -46,6 +46,7 @@ typedef struct or_outputs {
     int64_t   n_records;
     /* totals */
     int64_t total_steps, n_escaped, n_collisions, n_bound_launch;
+    int64_t n_drift_flagged;   /* hops that failed the energy-drift guard (dsmc_params.drift_tol) */
 } or_outputs;
 
 /* Philox4x32-10 block function (Salmon, Moraes, Dror, Shaw, SC'11). */

@@ -21,10 +21,11 @@ RNG_RAND_R, RNG_PHILOX = 0, 1
 
 
 def build(ref_root: str | None = None) -> None:
-    """Build liboracle.so; also oracle/_ref when the reference sources exist."""
+    """Build liboracle.so; also oracle/_ref when the reference sources exist: ref_root, else
+    $DSMC_REFERENCE_ROOT, else a checkout named `reference` beside this repository."""
     env = dict(os.environ)
     subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True, env=env)
-    ref = ref_root or os.environ.get("DSMC_REFERENCE_ROOT", "/root/reference")
+    ref = ref_root or os.environ.get("DSMC_REFERENCE_ROOT") or str(HERE.parent.parent / "reference")
     if Path(ref, "src", "dsmc", "ballistic.c").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True, env=env)
 
@@ -44,7 +45,7 @@ class Outputs(C.Structure):
         ("v_fd", C.POINTER(C.c_int32)), ("v_ht", C.POINTER(C.c_int32)),
         ("v_count_nn", C.POINTER(C.c_int32)), ("v_cap", C.c_int64), ("n_records", C.c_int64),
         ("total_steps", C.c_int64), ("n_escaped", C.c_int64), ("n_collisions", C.c_int64),
-        ("n_bound_launch", C.c_int64),
+        ("n_bound_launch", C.c_int64), ("n_drift_flagged", C.c_int64),
     ]
 
 
@@ -52,17 +53,20 @@ _lib = None
 
 
 def lib() -> C.CDLL:
+    """liboracle.so with its signatures. Structure arguments (dsmc_params, dsmc_surface,
+    dsmc_collision, ThermalParams) are passed by address, so callers may use the product's ctypes
+    structures (tests) or the oracle's own (oracle/problems.py, the timed CPU arm, which must not
+    load the product library)."""
     global _lib
     if _lib is None:
         if not LIB.exists():
             build()
-        from dsmc_suite_b200 import _native as N
         L = C.CDLL(str(LIB))
         D = C.POINTER(C.c_double)
+        V = C.c_void_p
         L.or_run.restype = C.c_int
-        L.or_run.argtypes = [C.POINTER(N.Params), C.POINTER(N.Surface), C.POINTER(N.Collision),
-                             C.POINTER(VTable), C.c_int, C.c_uint, C.c_int64, C.c_int64, C.c_int,
-                             C.POINTER(Outputs)]
+        L.or_run.argtypes = [V, V, V, C.POINTER(VTable), C.c_int, C.c_uint, C.c_int64, C.c_int64,
+                             C.c_int, C.POINTER(Outputs)]
         L.or_philox4x32.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                     C.POINTER(C.c_uint32)]
         L.or_verlet_step.restype = C.c_int
@@ -77,8 +81,7 @@ def lib() -> C.CDLL:
         L.or_cdf_sample.restype = C.c_double
         L.or_cdf_sample.argtypes = [D, D, C.c_double, C.c_int, C.c_double]
         L.or_thermal_solve.restype = C.c_int
-        L.or_thermal_solve.argtypes = [C.c_int, C.c_int, C.POINTER(N.ThermalParams), D, D,
-                                       C.POINTER(C.c_int)]
+        L.or_thermal_solve.argtypes = [C.c_int, C.c_int, V, D, D, C.POINTER(C.c_int)]
         L.or_shadow_flux.restype = C.c_int
         L.or_shadow_flux.argtypes = [C.c_int, D, C.c_int, C.POINTER(C.c_int32), D, C.c_double,
                                      C.c_int, C.c_int, D, C.c_int]
@@ -90,9 +93,13 @@ def lib() -> C.CDLL:
         L.or_fit_cell_from_hist.argtypes = [C.POINTER(C.c_uint64), C.c_int, C.c_double, C.c_int,
                                             D, D, D]
         L.or_locate_face.restype = C.c_int
-        L.or_locate_face.argtypes = [C.POINTER(N.Surface), D]
+        L.or_locate_face.argtypes = [V, D]
         _lib = L
     return _lib
+
+
+def _addr(struct) -> int | None:
+    return None if struct is None else C.addressof(struct)
 
 
 def _p(a, t=C.c_double):
@@ -120,7 +127,9 @@ def run(params, surface, n: int, collision=None, rng: int = RNG_PHILOX, rr_seed:
         particles: bool = True, v_record: bool = False, speed_hist: bool = False) -> dict:
     """Run the oracle over particles [pid_begin, pid_begin + n); returns numpy results.
 
-    surface / collision are dsmc_suite_b200._native.SurfaceInputs / CollisionInputs."""
+    params is a dsmc_params ctypes structure and surface / collision own a dsmc_surface /
+    dsmc_collision in their `.struct` (the product's SurfaceInputs / CollisionInputs, or
+    oracle.problems.SurfaceInputs)."""
     p = params
     ncell, nh = p.hd * p.ftd * p.ffd, p.ftd * p.ffd
     o = Outputs()
@@ -154,12 +163,13 @@ def run(params, surface, n: int, collision=None, rng: int = RNG_PHILOX, rr_seed:
         arr("v_count_nn", (p.ftd * p.hd,), np.int32, "v_count_nn", C.c_int32)
         o.v_cap = cap
     vt = vtable()
-    col = C.byref(collision.struct) if collision is not None else None
-    rc = lib().or_run(C.byref(p), C.byref(surface.struct), col, C.byref(vt), rng, rr_seed,
+    col = _addr(collision.struct) if collision is not None else None
+    rc = lib().or_run(_addr(p), _addr(surface.struct), col, C.byref(vt), rng, rr_seed,
                       pid_begin, n, nthreads, C.byref(o))
     if rc != 0:
         raise RuntimeError(f"or_run failed: {rc}")
-    for k in ("total_steps", "n_escaped", "n_collisions", "n_bound_launch", "n_records"):
+    for k in ("total_steps", "n_escaped", "n_collisions", "n_bound_launch", "n_drift_flagged",
+              "n_records"):
         res[k] = int(getattr(o, k))
     if v_record:
         k = res["n_records"]
@@ -174,7 +184,7 @@ def thermal(ftd: int, ffd: int, tp, flux: np.ndarray | None = None) -> tuple[np.
     F = None if flux is None else np.ascontiguousarray(flux, dtype=np.float64)
     T = np.zeros((ftd, ffd))
     h = C.c_int()
-    rc = lib().or_thermal_solve(ftd, ffd, C.byref(tp), _p(F) if F is not None else None, _p(T),
+    rc = lib().or_thermal_solve(ftd, ffd, _addr(tp), _p(F) if F is not None else None, _p(T),
                                 C.byref(h))
     if rc != 0:
         raise RuntimeError(f"or_thermal_solve failed: {rc}")

@@ -179,7 +179,7 @@ def test_icosphere_surface(N, O):
     for _ in range(3000):
         p = rng.normal(size=3)
         p /= np.linalg.norm(p)
-        assert ico.locate(p) == L.or_locate_face(C.byref(S.struct), O._p(np.ascontiguousarray(p)))
+        assert ico.locate(p) == L.or_locate_face(C.addressof(S.struct), O._p(np.ascontiguousarray(p)))
     T = ico.face_temperature(T_ss=235.0, T_floor=110.0)
     assert T.min() == 110.0 and 230 < T.max() <= 235.0
     cdf, rate = ico.source_cdf(T)
@@ -287,3 +287,42 @@ def test_no_device_fails_loudly(N):
 def test_cold_map_has_permanent_freeze_rows(N):
     T = cold_T(N)
     assert (T[:2] < 100).all() and (T[2:-2] >= 100).any(axis=1).all()
+
+
+def test_number_density_fp64_behind_the_c_abi(N):
+    """dsmc_number_density_host turns a fixed-point grid into molecules per m^3 in FP64; it must
+    agree with the host formula of workloads.number_density (physical volumes) and, with the
+    reference's volume convention, use the kept grid_compute_volume_* cells."""
+    from dsmc_suite_b200 import workloads as W
+    rng = np.random.default_rng(5)
+    for p in (N.params_config(N.RUNNER_BALLISTIC), N.params_config(N.RUNNER_ADVANCED, 1561e3, 3.2e12, 20),
+              N.params_reference(N.RUNNER_BALLISTIC, 36, 72), N.params_reference(N.RUNNER_ADVANCED, 36, 72)):
+        fx = rng.integers(0, 2**40, size=(p.hd, p.ftd, p.ffd), dtype=np.uint64)
+        fx[0, 0, :3] = 0
+        n, rate = 123457, 2.0e26
+        got = N.number_density(p, fx, n, rate)
+        want = W.number_density(p, fx, n, rate)
+        np.testing.assert_allclose(got, want, rtol=1e-13, atol=0)
+        assert (got[0, 0, :3] == 0).all()
+        # volumes: physical cells add up to the shell volume between R and max_height
+        vol = N.cell_volumes(p)
+        r_top = W.shell_radii(p)[-1]
+        assert abs(vol.sum() / (4.0 / 3.0 * np.pi * (r_top**3 - p.Radii**3)) - 1.0) < 1e-12
+        # the reference's own convention, through the kept entry points
+        vref = N.cell_volumes(p, N.VOLUME_REFERENCE)
+        g = N.SphericalGrid(ftd=p.ftd, ffd=p.ffd, hd=p.hd, volume=N.ptr(np.zeros(1)))
+        v2 = np.zeros(p.ncell)
+        g.volume = N.ptr(v2)
+        L = N.lib()
+        if p.use_exp_grid:
+            L.grid_compute_volume_exp(C.byref(g), C.c_double(p.Radii), C.c_double(p.unih),
+                                      C.c_double(p.alpha2))
+        else:
+            L.grid_compute_volume_uniform(C.byref(g), C.c_double(p.Radii), C.c_double(p.unih))
+        assert vref.ravel().tobytes() == v2.tobytes()
+        ref_nd = N.number_density(p, fx, n, rate, N.VOLUME_REFERENCE)
+        np.testing.assert_allclose(ref_nd * vref, got * vol, rtol=1e-13)
+    with pytest.raises(N.DsmcError):
+        N.number_density(p, fx, 0, rate)
+    with pytest.raises(N.DsmcError):
+        N.number_density(p, fx, n, rate, 7)

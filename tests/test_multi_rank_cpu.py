@@ -151,6 +151,95 @@ def test_two_rank_phase1_histograms_reduce_to_the_one_process_result(N, O, tmp_p
     assert red["hist"].sum() > 0
 
 
+def _phase2_inputs(N, O, p1, hist, density, n1):
+    """Phase-2 collision inputs from phase-1 results: the oracle's FP64 degree-6 fit of every
+    cell with more than 8 counts, the background from the weighted residence times. Every rank
+    calls it on the same reduced counts, so every rank holds the same tables."""
+    import ctypes as C
+    from dsmc_suite_b200 import workloads as W
+    ncell = p1.ncell
+    coef, box = np.zeros((ncell, N.CDF_STRIDE)), np.zeros((ncell, 4))
+    total, valid = np.zeros(ncell), np.zeros(ncell, dtype=np.int32)
+    L = O.lib()
+    for k in np.nonzero(hist.sum(axis=1) > 8)[0]:
+        h = np.ascontiguousarray(hist[k])
+        valid[k] = L.or_fit_cell_from_hist(h.ctypes.data_as(C.POINTER(C.c_uint64)), p1.n_speed_bins,
+                                           p1.speed_bin_width, 6, O._p(coef[k]), O._p(box[k]),
+                                           O._p(total[k:k + 1]))
+    nden = W.number_density(p1, density, n1, W.PRODUCTION_RATE)
+    col = N.CollisionInputs(nden.ravel(), W.fit_layout(p1, coef), W.fit_layout(p1, box),
+                            W.fit_layout(p1, total[:, None]).ravel(),
+                            W.fit_layout(p1, valid[:, None]).ravel(), 6)
+    p2 = N.params_config(N.RUNNER_ADVANCED)
+    p2.seed = p1.seed + 1
+    return p2, col
+
+
+def _two_phase_setup(N):
+    p1 = N.params_config(N.RUNNER_BALLISTIC)
+    p1.n_speed_bins = 64
+    ico = N.Icosphere(3)
+    return p1, N.SurfaceInputs(ico=ico, face_T=ico.face_temperature())
+
+
+def _rank_two_phase(rank, world, port, out_dir):
+    """Both phases of the collisional solve sharded by particle id: phase 1 on the rank's ids, one
+    all-reduce of density, horizon and histograms; the replicated fits; phase 2 on the rank's ids
+    against the fitted tables, one all-reduce of its grids."""
+    import sys
+    from datetime import timedelta
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    import torch.distributed as dist
+    from dsmc_suite_b200 import _native as N, shard
+    from oracle import oracle as O
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        p1, S = _two_phase_setup(N)
+        pid0, n = shard.particle_range(rank, world, N_PER_RANK)
+        r1 = O.run(p1, S, n, pid_begin=pid0, nthreads=2, particles=False, speed_hist=True)
+        den1, _, hist = shard.allreduce_grids(dist, r1["density"], r1["horizon"], r1["speed_hist"])
+        p2, col = _phase2_inputs(N, O, p1, hist, den1, world * N_PER_RANK)
+        r2 = O.run(p2, S, n, collision=col, pid_begin=pid0, nthreads=2, particles=False)
+        den2, hor2 = shard.allreduce_grids(dist, r2["density"], r2["horizon"])
+        ncol = shard.allreduce_grids(dist, np.array([r2["n_collisions"]], dtype=np.uint64))[0]
+        np.savez(os.path.join(out_dir, f"phase2_{rank}.npz"), density=den2, horizon=hor2,
+                 valid=col.valid, coef=col.coef, ncol=ncol)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_two_phase_solve_reduces_to_the_one_process_result(N, O, tmp_path):
+    """The collisional two-phase solve over two gloo ranks: the fits every rank replicates from the
+    reduced phase-1 counts are identical, and the reduced phase-2 grids (with collisions) equal one
+    process running both phases over all ids, bit for bit."""
+    import multiprocessing as mp
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_rank_two_phase, args=(r, world, port, str(tmp_path)))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    p1, S = _two_phase_setup(N)
+    n_all = world * N_PER_RANK
+    w1 = O.run(p1, S, n_all, nthreads=2, particles=False, speed_hist=True)
+    p2, col = _phase2_inputs(N, O, p1, w1["speed_hist"], w1["density"], n_all)
+    w2 = O.run(p2, S, n_all, collision=col, nthreads=2, particles=False)
+    assert w2["n_collisions"] > 0
+    for r in range(world):
+        got = np.load(tmp_path / f"phase2_{r}.npz")
+        np.testing.assert_array_equal(got["valid"], col.valid)
+        np.testing.assert_array_equal(got["coef"], col.coef)
+        np.testing.assert_array_equal(got["density"], np.asarray(w2["density"]).reshape(got["density"].shape))
+        np.testing.assert_array_equal(got["horizon"], np.asarray(w2["horizon"]).reshape(got["horizon"].shape))
+        assert int(got["ncol"][0]) == w2["n_collisions"]
+
+
 def test_two_rank_reduction_keeps_uint64_words(tmp_path):
     import multiprocessing as mp
     world = 2

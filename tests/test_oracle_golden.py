@@ -8,6 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import hashlib
 import subprocess
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -254,3 +255,62 @@ def test_thermal_oracle_matches_reference(N, O):
         live = O.reference_thermal(ftd, ffd, tp, flux)
         if live is not None:
             np.testing.assert_array_equal(T, live)
+
+
+def test_oracle_problem_setup_is_the_products_bit_for_bit(N):
+    """oracle/problems.py builds the CPU arm's inputs without the product library; they must be
+    the product's own parameter presets, icosphere and temperature fields, byte for byte."""
+    from oracle import problems as OP
+    for runner in (N.RUNNER_BALLISTIC, N.RUNNER_ADVANCED):
+        for ftd, ffd in ((36, 72), (18, 24)):
+            assert bytes(OP.params_reference(runner, ftd, ffd)) == \
+                bytes(N.params_reference(runner, ftd, ffd))
+        for R, GM, hd, seed in ((470e3, 6.26e10, 50, 20261203), (1561e3, 3.20e12, 20, 7),
+                                (1737e3, 4.90e12, 60, 2**63 + 5)):
+            assert bytes(OP.params_config(runner, R, GM, hd, seed)) == \
+                bytes(N.params_config(runner, R, GM, hd, seed))
+    for nlevel in (0, 1, 3):
+        a, b = OP.Icosphere(nlevel), N.Icosphere(nlevel)
+        for name in ("face_verts", "base_centroid", "split_planes"):
+            assert getattr(a, name).tobytes() == getattr(b, name).tobytes(), (nlevel, name)
+        for sun, T_ss in (((1.0, 0.0, 0.0), 235.0), ((0.6, 0.8, 0.0), 333.0)):
+            assert a.face_temperature(sun, T_ss, 110.0).tobytes() == \
+                b.face_temperature(sun, T_ss, 110.0).tobytes()
+    for sun in ((1.0, 0.0, 0.0), (0.0, 1.0, 0.0)):
+        assert OP.latlon_temperature(36, 72, sun, 235.0, 60.0).tobytes() == \
+            N.latlon_temperature(36, 72, sun, 235.0, 60.0).tobytes()
+
+
+def test_reference_arm_loads_only_oracle_libraries(tmp_path):
+    """The timed CPU arm of bench.py builds its workload with oracle/problems.py and runs the
+    oracle port: the product library must not be mapped into that process."""
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "import bench\n"
+            "r = bench.cpu_oracle_rate(0.2, 2, 300)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libdsmc_b200' not in maps, 'product library loaded'\n"
+            "assert 'liboracle.so' in maps\n"
+            "assert 'dsmc_suite_b200' not in sys.modules\n"
+            "print(r[2])\n" % str(ROOT))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT)
+    assert out.returncode == 0, out.stderr
+    assert int(out.stdout.split()[-1]) > 0
+
+
+def test_oracle_energy_drift_guard(O):
+    """The per-hop energy-drift guard of the oracle: the config workloads' hops at dt = 2 s stay
+    inside drift_tol * GM / R (the reference's integrator drifts by ~1e-3 GM / R over a hop), a
+    ten times larger step flags many hops, and drift_tol = 0 turns the count off."""
+    import math
+    from oracle import problems as OP
+    ico = OP.Icosphere(3)
+    S = OP.SurfaceInputs(ico=ico, face_T=ico.face_temperature())
+    for R, GM in ((470e3, 6.26e10), (1737e3, 4.90e12)):
+        p = OP.params_config(OP.RUNNER_BALLISTIC, R, GM, 50, 11)
+        assert O.run(p, S, 1500, nthreads=4, particles=False)["n_drift_flagged"] == 0
+        p.dt_step = 20.0
+        p.wdecay = math.exp(-p.dt_step / p.lifetime)
+        big = O.run(p, S, 1500, nthreads=4, particles=False)
+        assert big["n_drift_flagged"] > 500
+        p.drift_tol = 0.0
+        assert O.run(p, S, 300, nthreads=4, particles=False)["n_drift_flagged"] == 0

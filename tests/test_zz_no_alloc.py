@@ -30,19 +30,34 @@ def _dptr(t, ctype=C.c_double):
     return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ctype))
 
 
-def _noalloc_solve(N, torch, p, surf_dev, n):
-    ncell, nh = p.ncell, p.ftd * p.ffd
-    density = torch.zeros(ncell, dtype=torch.int64, device="cuda")
-    horizon = torch.zeros(nh, dtype=torch.int64, device="cuda")
-    stats = torch.full((6,), 7, dtype=torch.int64, device="cuda")   # the call must zero these
+def _buffers(torch, p):
+    """Device buffers the caller owns: density, horizon and the six statistics words (set to a
+    non-zero pattern, which the call must clear)."""
+    return (torch.zeros(p.ncell, dtype=torch.int64, device="cuda"),
+            torch.zeros(p.ftd * p.ffd, dtype=torch.int64, device="cuda"),
+            torch.full((6,), 7, dtype=torch.int64, device="cuda"))
+
+
+def _call(N, p, surf_dev, n, bufs):
+    density, horizon, stats = bufs
     rc = N.lib().dsmc_solve_fast_noalloc(C.byref(p), C.byref(surf_dev), 0, n,
                                          _dptr(density, C.c_uint64), _dptr(horizon, C.c_uint64),
                                          _dptr(stats, C.c_uint64), None)
     assert rc == 0, N.lib().dsmc_noalloc_last_error()
-    torch.cuda.synchronize()
+
+
+def _host(p, bufs):
+    density, horizon, stats = bufs
     return (density.cpu().numpy().view(np.uint64).reshape(p.hd, p.ftd, p.ffd),
             horizon.cpu().numpy().view(np.uint64).reshape(p.ftd, p.ffd),
             stats.cpu().numpy())
+
+
+def _noalloc_solve(N, torch, p, surf_dev, n):
+    bufs = _buffers(torch, p)
+    _call(N, p, surf_dev, n, bufs)
+    torch.cuda.synchronize()
+    return _host(p, bufs)
 
 
 def test_noalloc_matches_existing_entry_point_twice(N, built):
@@ -80,6 +95,42 @@ def test_noalloc_matches_existing_entry_point_twice(N, built):
         assert int(s[0]) == st["total_steps"] > 0
         assert int(s[1]) == st["n_escaped"] and int(s[4]) == st["n_finished"] == n
 
+    # A third call allocates no device memory: the device's free memory is the same before and
+    # after it (its buffers are the caller's, allocated beforehand).
+    bufs = _buffers(torch, pc)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    _call(N, pc, sd, n1, bufs)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0, "the no-allocation call allocated device memory"
+    d3, h3, _ = _host(pc, bufs)
+    np.testing.assert_array_equal(d3, ref1["density"])
+    np.testing.assert_array_equal(h3, ref1["horizon"])
+
+
+def test_noalloc_long_lived_particles(N, built):
+    """A few reference-model particles that live for 9e6 steps each (no photolysis, no escape by
+    launch speed, a 9e6-step life cap): the tail of the solve runs more than a thousand launches
+    in which no particle finishes, which must not read as a stalled queue; the result equals the
+    existing entry point's."""
+    torch = pytest.importorskip("torch")
+    from dsmc_suite_b200 import Context
+    p = N.params_reference(N.RUNNER_BALLISTIC, 36, 72)
+    p.ve, p.lifetime, p.wdecay, p.w_min = 1e30, 1e30, 1.0, -1.0
+    p.life_step_cap = 9_000_000
+    T = N.latlon_temperature(36, 72, T_ss=235.0, T_floor=110.0)
+    Td = _dev(torch, T)
+    sr = N.Surface()
+    sr.T_map = _dptr(Td)
+    n = 8
+    d, h, s = _noalloc_solve(N, torch, p, sr, n)
+    with Context(0) as ctx:
+        ref = ctx.solve(N.PATH_FAST_FP32, p, N.SurfaceInputs(T_map=T), n)
+    np.testing.assert_array_equal(d, ref["density"])
+    np.testing.assert_array_equal(h, ref["horizon"])
+    assert int(s[0]) == ref["stats"]["total_steps"] and int(s[4]) == n
+    assert int(s[0]) > 9_000_000, "no particle reached the life cap"
+
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(N, built):
     pytest.importorskip("torch")
@@ -89,3 +140,12 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(N, built):
     rc = N.lib().dsmc_solve_fast_noalloc(C.byref(p), C.byref(s), 0, 10, dummy, dummy, dummy, None)
     assert rc == -1
     assert b"too large" in N.lib().dsmc_noalloc_last_error()
+    p2 = N.params_config(N.RUNNER_BALLISTIC)
+    p2.model = 5
+    assert N.lib().dsmc_solve_fast_noalloc(C.byref(p2), C.byref(s), 0, 10, dummy, dummy, dummy, None) == -1
+    assert b"unknown physics model" in N.lib().dsmc_noalloc_last_error()
+    p3 = N.params_config(N.RUNNER_BALLISTIC)
+    for pid0, n in ((2**32 - 5, 10), (2**62, 2**62), (0, 2**32 + 1)):
+        assert N.lib().dsmc_solve_fast_noalloc(C.byref(p3), C.byref(s), pid0, n, dummy, dummy, dummy,
+                                               None) == -1
+        assert b"[0, 2^32)" in N.lib().dsmc_noalloc_last_error()
