@@ -220,3 +220,30 @@ def shadow_flux(spot, facet, normal, za: float, tt: int, nmonte: int, nthreads: 
     if rc != 0:
         raise RuntimeError(f"or_shadow_flux failed: {rc}")
     return F
+
+
+def reference_shadow_flux(spot, facet, za_deg: float, tt: int, nmonte: int, workdir,
+                          nthreads: int = 8):
+    """The reference's own ray tracer, run_raytracer of src/raytracer/shadow_maker.c compiled
+    unmodified into oracle/_ref/libshadowref.so against the brute-force Embree stand-in of
+    oracle/embree_shim/. Writes the mesh files it reads (vertices, 1-based face triples), runs it
+    and returns its flux file as F [nface][tt] (printed %9.7f), or None when that build is absent."""
+    from pathlib import Path
+    so = REF_DIR / "libshadowref.so"
+    if not so.exists():
+        return None
+    spot = np.ascontiguousarray(spot, dtype=np.float64)
+    facet = np.ascontiguousarray(facet, dtype=np.int64)
+    d = Path(workdir)
+    (d / "ref_vert.txt").write_text("".join(f"{x:.17g} {y:.17g} {z:.17g}\n" for x, y, z in spot))
+    (d / "ref_face.txt").write_text("".join(f"{a + 1} {b + 1} {c + 1}\n" for a, b, c in facet))
+    R = C.CDLL(str(so))
+    R.run_raytracer.restype = None
+    R.run_raytracer.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int,
+                                C.c_int, C.c_char_p, C.c_int]
+    out = d / "ref_flux.dat"
+    R.run_raytracer(str(d / "ref_vert.txt").encode(), str(d / "ref_face.txt").encode(),
+                    spot.shape[0], facet.shape[0], za_deg, tt, nmonte, str(out).encode(), nthreads)
+    vals = out.read_text().split()
+    assert int(vals[0]) == facet.shape[0] and int(vals[1]) == tt
+    return np.array(vals[2:], dtype=np.float64).reshape(facet.shape[0], tt)

@@ -9,6 +9,7 @@ from __future__ import annotations
 import ctypes as C
 
 import numpy as np
+import pytest
 
 
 def _sun(za, tt):
@@ -73,3 +74,20 @@ def test_kept_mesh_entry_points(N, tmp_path):
     r2 = libc.rand_r(C.byref(s2)) / 2147483647.0
     assert (p.x, p.y, p.z) == (1.0 - r1, r1 * (1.0 - r2), r1 * r2)
     assert s1.value == s2.value
+
+
+def test_oracle_matches_the_reference_ray_tracer(N, O, tmp_path):
+    """The reference's own shadow_maker.c (run_raytracer, compiled unmodified against the
+    brute-force Embree stand-in of oracle/embree_shim/) pins the oracle's sampling, occlusion
+    rays and flux arithmetic: its flux file equals the oracle's flux to the printed precision."""
+    from dsmc_suite_b200 import workloads as W
+    spot, facet = W.cratered_mesh(3, depth=0.3)
+    za_deg, tt, nmonte = 17.0, 6, 16
+    ref = O.reference_shadow_flux(spot, facet, za_deg, tt, nmonte, tmp_path)
+    if ref is None:
+        pytest.skip("oracle/_ref/libshadowref.so not built (reference sources absent)")
+    n = N.mesh_normals(spot, facet)["normal"]
+    F = O.shadow_flux(spot, facet, n, za_deg / 180.0 * np.pi, tt, nmonte)
+    np.testing.assert_allclose(F, ref, atol=6e-8, rtol=0)
+    c6 = np.where(n @ _sun(za_deg / 180.0 * np.pi, tt).T < 0, 0.0, n @ _sun(za_deg / 180.0 * np.pi, tt).T)
+    assert np.mean(ref < c6 - 1e-6) > 0.01        # shadows were cast and matched
