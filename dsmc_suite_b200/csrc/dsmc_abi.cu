@@ -241,14 +241,13 @@ int dsmc_run(dsmc_ctx *c, int path, int64_t pid_begin, int64_t n) {
             c->last_launches = n > 0 ? 1 : 0;
             return DSMC_OK;
         case DSMC_PATH_FAST_FP64:
-            return fail(c, DSMC_ERR_INVALID,
-                        "FAST_FP64 is reserved and not built: the FP64 solve is PLAIN_FP64");
         case DSMC_PATH_FAST_FP32: {
             if (!c->fast) {
                 c->fast = new (std::nothrow) dsmc::FastEngine();
                 if (!c->fast) return fail(c, DSMC_ERR_NO_MEMORY, "host allocation failed");
             }
-            cudaError_t e = c->fast->run(c->params, c->t, false, pid_begin, n, c->num_sms, c->stream);
+            cudaError_t e = c->fast->run(c->params, c->t, path == DSMC_PATH_FAST_FP64, pid_begin, n,
+                                         c->num_sms, c->stream);
             c->last_launches = c->fast->launches;
             if (e != cudaSuccess)
                 return fail(c, e == cudaErrorMemoryAllocation ? DSMC_ERR_NO_MEMORY : DSMC_ERR_CUDA,

@@ -19,11 +19,15 @@ struct FastInst {
     const float *rb2;        // [hd+1] squared shell boundaries, rb2[0] = R^2, rb2[hd] = r_top^2
     const float *sbs;        // [ftd+1] sin(b)|sin(b)| of latitude boundaries b_k
     const float2 *lonb;      // [ffd+1] (sin, cos) of longitude boundaries phi_k = 2 pi k / ffd
+    // the same boundary tables in FP64 (FAST_FP64 solves; nullptr elsewhere)
+    const double *rb2d, *sbsd;
+    const double2 *lonbd;
     long long work_base;     // first work index of this instance in the queue
     long long n;             // particles
     long long pid_begin;     // particle id of the first particle
     float c_day;             // h / lifetime / ln 2 (W = W0 * 2^(-c_day * n_day))
     float r_land2, r_esc2;   // Radii^2, max_height^2
+    double c_day_d;          // c_day in FP64
     double drift_abs;        // drift_tol * GM / Radii: the energy-drift guard's bound (0 = off)
     const float4 *face_f;    // FP32 icosphere tables (config model), or nullptr: FP64 descent
 };
@@ -34,35 +38,42 @@ size_t face_floats_for(int nlevel);
 size_t face_table_floats(const dsmc_params &p, const DevTables &t);
 cudaError_t build_face_tables(const DevTables &t, float4 *out, cudaStream_t stream);
 
-// Structure-of-arrays particle slots.
-struct Slots {
+// Structure-of-arrays particle slots of an engine computing in R: float (the FAST_FP32 path:
+// position and velocity as two-sum (hi, lo) pairs) or double (FAST_FP64: the lo arrays are
+// carved but unused).
+template <typename R>
+struct SlotsT {
     int *inst;               // instance index, -1 = empty
     unsigned *pid;           // particle id within its instance
     unsigned *evt;           // Philox event counter
-    float *sh, *sl, *vh, *vl, *oa;   // [3][S] each: position hi/lo, velocity hi/lo, old accel
-    float *w0;               // weight factor outside photolysis
+    R *sh, *sl, *vh, *vl, *oa;   // [3][S] each: position hi/lo, velocity hi/lo, old accel
+    R *w0;                   // weight factor outside photolysis
     int *nday;               // day-side steps (photolysis exponent)
     int *steps;              // steps in the particle's life
     int *hop;                // steps in the current hop
     int *cell;               // packed (ht << 16) | (td << 8) | fd
     int *run_cell;           // cell of the register deposit run, -1 = none
-    float *run_w;            // weight-steps in run_cell not yet flushed (8-byte slot reserved)
+    R *run_w;                // weight-steps in run_cell not yet flushed (8-byte slot reserved)
     int *hist_key;           // (cell * nbins + bin) of the speed-histogram run, -1 = none
     int *hist_cnt;
-    float *pcol, *pthr;      // accumulated collision probability and its threshold
+    R *pcol, *pthr;          // accumulated collision probability and its threshold
     int *ncol;
     float *rest;             // freeze waiting time (reference model)
-    float *wcur;             // running weight (the hot loop's W between launches)
+    R *wcur;                 // running weight (the hot loop's W between launches)
     int *face;               // icosphere face of the last launch point (config model), -1 = none
     float *e0;               // orbital energy at the hop's launch or last collision (drift guard)
 };
+using Slots = SlotsT<float>;
 
-// Bytes of one slot in the structure-of-arrays block: run_w (8-byte slot) plus 33 four-byte
-// fields (inst pid evt, 15 vector floats, w0 nday steps hop cell run_cell hist_key hist_cnt pcol
-// pthr ncol rest wcur face e0). carve_slots lays the arrays out in that order over slot memory of
-// fast_slot_bytes(nslots) bytes.
-constexpr size_t kSlotBytesPerSlot = 33 * 4 + 8;
-Slots carve_slots(void *mem, long long nslots);
+// Bytes of one slot in the structure-of-arrays block: run_w (an 8-byte slot), the 4-byte fields
+// (inst pid evt nday steps hop cell run_cell hist_key hist_cnt ncol rest face e0) and the R fields
+// (15 vector components, w0, pcol, pthr, wcur). carve_slots lays the arrays out over slot memory
+// of fast_slot_bytes(nslots) bytes; nslots a multiple of 128 keeps every array 512-byte aligned.
+template <typename R>
+constexpr size_t slot_bytes_per_slot() { return 8 + 14 * 4 + 19 * sizeof(R); }
+constexpr size_t kSlotBytesPerSlot = slot_bytes_per_slot<float>();
+template <typename R>
+SlotsT<R> carve_slots(void *mem, long long nslots);
 
 // Device-side queue state. `total` and `ninst` live here rather than in the kernel arguments so
 // that the host can append instances between launches of an already captured graph.
@@ -80,7 +91,7 @@ struct FastCounters {
 // launch loop without graphs on caller memory until the queue of `total` particles is empty, and
 // gives up (cudaErrorLaunchTimeout) after stall_launches launches in a row in which no particle
 // finished.
-size_t fast_slot_bytes(long long nslots);
+size_t fast_slot_bytes(long long nslots, bool fp64 = false);
 size_t fast_inst_bytes();
 size_t fast_counter_bytes();
 cudaError_t fast_fill_instance(const dsmc_params &p, const DevTables &t, long long pid_begin,
@@ -98,7 +109,9 @@ public:
     FastEngine(const FastEngine &) = delete;
     FastEngine &operator=(const FastEngine &) = delete;
 
-    // Solve particles [pid_begin, pid_begin + n) of one instance to the end of their lives.
+    // Solve particles [pid_begin, pid_begin + n) of one instance to the end of their lives, in
+    // FP32 with two-sum compensation (fp64 false) or in FP64 (the FAST_FP64 path: the same
+    // slots, queue, cell tracking and register deposits on double state and FP64 tables).
     cudaError_t run(const dsmc_params &p, const DevTables &t, bool fp64, long long pid_begin,
                     long long n, int num_sms, cudaStream_t stream);
 
@@ -132,6 +145,7 @@ private:
     cudaError_t prepare_graph(cudaStream_t stream);
     cudaError_t capture(cudaStream_t stream, int mode, cudaGraphExec_t *out);
     cudaError_t round(cudaStream_t stream);
+    void launch_kernel(cudaStream_t stream, int mode, unsigned grid);   // one launch, fp64_ state
 
 public:
     // Serving: an open queue that grows while it drains. serve_open resets the engine to an
@@ -170,7 +184,10 @@ private:
     void free_all();
 
     Slots slots_{};
+    SlotsT<double> slots64_{};                // the same memory carved for FP64 state
     void *slot_mem_ = nullptr;
+    bool fp64_ = false;                       // precision of run / run_batch launches
+    bool slot_fp64_ = false;                  // precision the slot memory is carved for
     long long nslots_ = 0;
     FastInst *d_inst_ = nullptr;
     int ninst_cap_ = 0;

@@ -24,6 +24,7 @@ static int env_path(void)
     const char *v = getenv("DSMC_PATH");
     if (!v || !*v || !strcmp(v, "plain")) return DSMC_PATH_PLAIN_FP64;
     if (!strcmp(v, "fast32") || !strcmp(v, "fast")) return DSMC_PATH_FAST_FP32;
+    if (!strcmp(v, "fast64")) return DSMC_PATH_FAST_FP64;
     return DSMC_PATH_PLAIN_FP64;
 }
 

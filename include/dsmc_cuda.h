@@ -90,8 +90,11 @@ typedef struct dsmc_ctx dsmc_ctx;
  * the reference's FP64 arithmetic without FMA contraction, one atomic per deposited step.
  * FAST_FP32 keeps resident particle slots that refill from a work queue, pushes in FP32 with
  * two-sum compensated positions and velocities, tracks cells by comparisons, and aggregates
- * deposits in registers. FAST_FP64 is reserved (not built; dsmc_run rejects it with
- * DSMC_ERR_INVALID): the FP64 solve is PLAIN_FP64, which follows the reference's arithmetic. */
+ * deposits in registers. FAST_FP64 is the same resident-slot engine on FP64 state and FP64
+ * boundary tables (no compensation needed), with the plain path's FP64 maps of the random words
+ * at launches and collisions: it follows the same Philox streams as PLAIN_FP64 and differs from
+ * it only by rounding, so it serves as the full-size FP64 reference of FAST_FP32. FAST_FP64
+ * runs 128-thread blocks; other launch shapes are FAST_FP32 only. */
 enum dsmc_path { DSMC_PATH_PLAIN_FP64 = 0, DSMC_PATH_FAST_FP32 = 1, DSMC_PATH_FAST_FP64 = 2 };
 
 typedef struct dsmc_stats {

@@ -5,10 +5,12 @@
  * files, solve on the GPU through include/dsmc_cuda.h and write the same output files:
  *   <prefix>_den.dat, <prefix>_horizon.dat, <prefix>_v_record.dat (ballistic), <prefix>_ttime.dat
  * nthreads is accepted for compatibility; the solve runs on one CUDA device (DSMC_DEVICE,
- * default 0). DSMC_PATH selects the kernel path (plain or fast32; default plain) and DSMC_SEED
- * the Philox seed. DSMC_SIDECAR=1 (the CLI's --bin) also writes <prefix>_grids.bin, the exact
+ * default 0). DSMC_PATH selects the kernel path (plain, fast32 or fast64; default plain) and
+ * DSMC_SEED the Philox seed. DSMC_SIDECAR=1 (the CLI's --bin) also writes <prefix>_grids.bin, the exact
  * fixed-point grids and FP64 per-particle rows (layout in fileio.h / host_fileio.c). On failure
- * a message goes to stderr and no file is written. */
+ * a message goes to stderr and no file is written. DSMC_NDENSITY_RATE=Q (the CLI's --ndensity Q)
+ * also writes <prefix>_ndensity.dat, the FP64 number density [m^-3] for a production rate of
+ * Q molecules/s (dsmc_number_density_host, physical cell volumes). */
 #ifndef DSMC_RUNNERS_H
 #define DSMC_RUNNERS_H
 
