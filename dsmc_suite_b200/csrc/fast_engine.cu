@@ -1827,7 +1827,8 @@ cudaError_t FastEngine::drain(long long total, cudaStream_t stream) {
     h_ctr_->ninst = ninst_;
     if ((e = cudaMemcpyAsync(d_ctr_, h_ctr_, sizeof(FastCounters), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return e;
-    if ((e = cudaMemsetAsync(slots_.inst, 0xff, nslots_ * sizeof(int), stream)) != cudaSuccess) return e;
+    int *inst = slot_fp64_ ? slots64_.inst : slots_.inst;
+    if ((e = cudaMemsetAsync(inst, 0xff, nslots_ * sizeof(int), stream)) != cudaSuccess) return e;
     if (launches_per_graph > 1 && (e = prepare_graph(stream)) != cudaSuccess) return e;
     // Every launch advances each live particle by K steps or ends it, and every life is bounded
     // by its step caps, so the queue drains. The loop still gives up (launch-timeout status) if
