@@ -279,7 +279,8 @@ def test_runner_files_match_oracle(N, O, tmp_path, built):
     cli = ROOT / "dsmc_suite_b200" / "bin" / "dsmc_suite"
     n = 300
     r = subprocess.run([str(cli), "dsmc", "-n", str(n), "-T", str(tmp_path / "T.dat"), "-o",
-                        str(tmp_path / "g"), "--bin"], capture_output=True, text=True)
+                        str(tmp_path / "g"), "--bin", "--ndensity", "2e26"],
+                       capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert "Simulation complete" in r.stdout
     p = N.params_reference(N.RUNNER_BALLISTIC, 36, 72)
@@ -291,6 +292,11 @@ def test_runner_files_match_oracle(N, O, tmp_path, built):
     lines = (tmp_path / "g_den.dat").read_text().split("\n")[3:-1]
     assert lines == ["%9.6f" % x for x in g["density"] / g["fixed_scale"]]
     assert np.mean(g["density"] == o["density"].ravel()) >= 0.999
+    # --ndensity: the FP64 number density of the same grid, m^-3
+    nd = np.array((tmp_path / "g_ndensity.dat").read_text().split(), dtype=np.float64)
+    assert nd[:3].tolist() == [36, 72, p.hd]
+    want = N.number_density(p, g["density"].reshape(p.hd, 36, 72), n, 2e26)
+    np.testing.assert_allclose(nd[3:], want.ravel(), rtol=1e-9, atol=0)
     assert np.mean(g["horizon"] == o["horizon"].ravel()) >= 0.99
     same = np.all(np.isclose(g["ttime"], o["ttime"][:5], rtol=1e-9, atol=1e-6), axis=0)
     assert same.mean() >= 0.995, same.mean()
