@@ -94,7 +94,7 @@ typedef struct dsmc_ctx dsmc_ctx;
  * boundary tables (no compensation needed), with the plain path's FP64 maps of the random words
  * at launches and collisions: it follows the same Philox streams as PLAIN_FP64 and differs from
  * it only by rounding, so it serves as the full-size FP64 reference of FAST_FP32. FAST_FP64
- * runs 128-thread blocks; other launch shapes are FAST_FP32 only. */
+ * runs 128-thread blocks, 4 (default) or 3 resident per SM. */
 enum dsmc_path { DSMC_PATH_PLAIN_FP64 = 0, DSMC_PATH_FAST_FP32 = 1, DSMC_PATH_FAST_FP64 = 2 };
 
 typedef struct dsmc_stats {
