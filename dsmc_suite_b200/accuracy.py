@@ -12,6 +12,14 @@ its solve follows the same Philox streams as the FP32 path. Reported:
     relative L2 between two independent FP32 solves (the Monte Carlo noise at this N);
   * column density at impact parameters 1.1, 1.5, 2, 3, 5 and 8 R for both paths.
 Prints one JSON line; --md also writes a markdown summary.
+
+    python -m dsmc_suite_b200.accuracy --agreement [--particles 1e5] [--md out.md]
+
+instead compares the three paths on the same Philox streams over five workloads (the Ceres-,
+Europa- and Moon-like ballistic bodies, the reference model on a 36 x 72 map, the config-model
+collisional phase 2 with degree-6 fits): per path against PLAIN_FP64, the fraction of particles
+with the same fate and step count and the density relative L2, beside the relative L2 between two
+independent PLAIN_FP64 runs.
 """
 from __future__ import annotations
 
@@ -95,6 +103,66 @@ def density_errors(ctx: Context, p: N.Params, surf, n: int) -> dict:
                                    (cd["fp32_other_seed"] / cd["fp32"] - 1).tolist()}}
 
 
+def agreement(ctx: Context, n: int) -> dict:
+    """FAST_FP64 and FAST_FP32 against PLAIN_FP64 on five workloads, same Philox streams."""
+    surf = W.config_surface()
+    cases = []
+    for body in ("ceres", "europa", "moon"):
+        R, GM = W.BODIES[body]
+        cases.append((body, N.params_config(N.RUNNER_BALLISTIC, R, GM, 50, 20261203), surf, None, n))
+    T = N.latlon_temperature(36, 72, T_ss=235.0, T_floor=60.0)
+    cases.append(("reference", N.params_reference(N.RUNNER_BALLISTIC, 36, 72), N.SurfaceInputs(T_map=T),
+                  None, max(1000, n // 3)))
+    prob = W.collisional_problem(ctx, "collisional", 470e3, 6.26e10, 50, 20261203, W.sun_vector(0.0),
+                                 235.0, n, n, path=N.PATH_PLAIN_FP64)
+    cases.append(("collisional", prob.params, prob.surface, prob.collision, n))
+    out = {}
+    for name, p, S, col, m in cases:
+        r = {path: ctx.solve(path, p, S, m, collision=col, outputs=True)
+             for path in (N.PATH_PLAIN_FP64, N.PATH_FAST_FP64, N.PATH_FAST_FP32)}
+        q = p.copy()
+        q.seed = p.seed + 1
+        ind = ctx.solve(N.PATH_PLAIN_FP64, q, S, m, collision=col)["density"]
+        a = r[N.PATH_PLAIN_FP64]
+        row = {"particles": m, "noise_rel_l2": W.rel_l2(ind, a["density"]),
+               "steps_plain": a["stats"]["total_steps"], "collisions_plain": a["stats"]["n_collisions"],
+               "drift_flagged_plain": a["stats"]["n_drift_flagged"]}
+        for path, key in ((N.PATH_FAST_FP64, "fast_fp64"), (N.PATH_FAST_FP32, "fast_fp32")):
+            b = r[path]
+            row[key] = {"same_fate_and_steps": float(np.mean((b["fate"] == a["fate"]) & (b["steps"] == a["steps"]))),
+                        "same_fate": float(np.mean(b["fate"] == a["fate"])),
+                        "density_rel_l2": W.rel_l2(b["density"], a["density"]),
+                        "steps_ratio": b["stats"]["total_steps"] / max(a["stats"]["total_steps"], 1),
+                        "collisions": b["stats"]["n_collisions"],
+                        "drift_flagged": b["stats"]["n_drift_flagged"]}
+        out[name] = row
+    return out
+
+
+def agreement_markdown(res: dict, cmd: str) -> str:
+    rows = []
+    for name, r in res.items():
+        for key in ("fast_fp64", "fast_fp32"):
+            x = r[key]
+            rows.append(f"| {name} | {r['particles']} | {key.upper()} | {100 * x['same_fate']:.3f} % | "
+                        f"{100 * x['same_fate_and_steps']:.3f} % | {x['density_rel_l2']:.2e} | "
+                        f"{r['noise_rel_l2']:.2e} | {x['steps_ratio']:.6f} | {x['collisions']} "
+                        f"({r['collisions_plain']}) | {x['drift_flagged']} ({r['drift_flagged_plain']}) |")
+    return f"""# FAST_FP64 and FAST_FP32 against PLAIN_FP64, same Philox streams
+
+Command: `{cmd}`
+
+PLAIN_FP64 reproduces the oracle, which reproduces the reference binary (rand_r mode). Columns:
+particles with the same fate as PLAIN_FP64; with the same fate and step count; per-cell density
+relative L2 against PLAIN_FP64; the same between two independent PLAIN_FP64 runs (Monte Carlo
+noise); particle-steps relative to PLAIN_FP64; collisions and drift-flagged hops (PLAIN_FP64's in
+brackets).
+
+| workload | particles | path | same fate | same fate and steps | density rel-L2 | noise rel-L2 | steps ratio | collisions | drift-flagged hops |
+|---|---|---|---|---|---|---|---|---|---|
+""" + "\n".join(rows) + "\n"
+
+
 def markdown(res: dict, cmd: str) -> str:
     e, d = res["endpoint"], res["density"]
     cd = d["column_density"]
@@ -138,8 +206,17 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--md", type=str, default=None)
+    ap.add_argument("--agreement", action="store_true")
     args = sys.argv[1:] if argv is None else argv
     a = ap.parse_args(args)
+    if a.agreement:
+        with Context(a.device) as ctx:
+            res = agreement(ctx, int(a.particles) if a.particles != 1e8 else 100_000)
+        print(json.dumps(res), flush=True)
+        if a.md:
+            with open(a.md, "w") as f:
+                f.write(agreement_markdown(res, "python -m dsmc_suite_b200.accuracy " + " ".join(args)))
+        return
     p = N.params_config(N.RUNNER_BALLISTIC, 470e3, 6.26e10, 50, 20261203)
     surf = W.config_surface()
     with Context(a.device) as ctx:
