@@ -51,6 +51,8 @@ def args_parse():
     ap.add_argument("--shape", type=str, default=None,
                     help="launch shape block,blocks_per_sm,steps_per_launch,launches_per_graph")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--solver", choices=["fast32", "fast64"], default="fast32",
+                    help="solve: the timed path (FAST_FP32, the default, or the FP64 engine FAST_FP64)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", choices=["solve", "batch", "serve", "collisional", "thermal",
                                        "raytrace"], default="solve",
@@ -754,9 +756,11 @@ def main():
     red = torch.zeros(ncell + nh, dtype=torch.int64, device="cuda") if world > 1 else None
     L = N.lib()
 
+    timed_path = N.PATH_FAST_FP64 if a.solver == "fast64" else N.PATH_FAST_FP32
+
     def solve_step():
         ctx.zero()
-        ctx.run(N.PATH_FAST_FP32, pid0, n)
+        ctx.run(timed_path, pid0, n)
         if red is not None:
             d_ptr = red.data_ptr()
             N.check(L.dsmc_copy_grids_device(ctx.h, C_u64(d_ptr), C_u64(d_ptr + 8 * ncell)), "copy", ctx.h)
@@ -806,8 +810,9 @@ def main():
     per_rank_rate = steps_done / (t_ms * 1e-3)
 
     # roofline of the push kernel: algorithmic FP ops / time against the measured FP32 FMA peak
+    fp64_timed = a.solver == "fast64"
     peak = ctypes.c_double()
-    N.check(L.dsmc_measure_fma_peak(ctx.h, 0, ctypes.byref(peak)), "fma peak", ctx.h)
+    N.check(L.dsmc_measure_fma_peak(ctx.h, 1 if fp64_timed else 0, ctypes.byref(peak)), "fma peak", ctx.h)
     achieved = per_rank_rate * FLOPS_PER_STEP / 1e12
     traffic = None
     prof = ROOT / "profiles" / "fast_kernel_traffic.json"
@@ -815,16 +820,19 @@ def main():
         tj = json.loads(prof.read_text())
         # DRAM bytes per particle-step from the ncu capture, scaled to this run's launches
         traffic = tj["dram_bytes_per_step"] * (steps_done / launches)
-    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
-                "peak_source": "measured in this run: FP32 FMA-chain kernel "
-                               "(dsmc_measure_fma_peak)",
+    roofline = {"bound": "fp64" if fp64_timed else "fp32", "achieved": achieved, "peak": peak.value,
+                "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None,
+                "traffic": None if fp64_timed else traffic,
+                "peak_source": f"measured in this run: {'FP64' if fp64_timed else 'FP32'} FMA-chain "
+                               "kernel (dsmc_measure_fma_peak)",
                 "algorithmic_flops_per_step": FLOPS_PER_STEP}
 
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_ms / a.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-            "data": "synthetic", "config": workload_config(n, world), "solver": SOLVER,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if fp64_timed else "fp32",
+            "data": "synthetic", "config": workload_config(n, world),
+            "solver": "FAST_FP64 resident slots, FP64 push" if fp64_timed else SOLVER,
             "particle_steps_per_step": steps_all / a.steps, "gpu_launches": launches,
             "resident_slots": nslots, "clocks": clocks.summary(), "roofline": roofline}
 
@@ -850,6 +858,7 @@ def main():
         line["plain_fp64"] = {"value": plain, "unit": METRIC, "particles": npl,
                               "fp64_fma_peak_tflops": pk64.value}
         line["speedup_vs_plain_fp64"] = value / plain
+    if rank == 0 and world == 1 and not fp64_timed:
         # the FP64 resident-slot engine on the whole workload (same streams): what the FP32
         # compensated push buys over the same engine in FP64, and the FP32 result's error at
         # full size against it
@@ -889,7 +898,7 @@ def main():
         pe = p.copy()
 
         def solve_host():
-            N.check(L.dsmc_solve_host(ctx2.h, N.PATH_FAST_FP32, ctypes.byref(pe),
+            N.check(L.dsmc_solve_host(ctx2.h, timed_path, ctypes.byref(pe),
                                       ctypes.byref(S_pin.struct), None, n,
                                       N.ptr(den_h, ctypes.c_uint64), N.ptr(hor_h, ctypes.c_uint64),
                                       ctypes.byref(stats)), "solve_host", ctx2.h)
