@@ -28,6 +28,8 @@ struct FastInst {
     float c_day;             // h / lifetime / ln 2 (W = W0 * 2^(-c_day * n_day))
     float r_land2, r_esc2;   // Radii^2, max_height^2
     double c_day_d;          // c_day in FP64
+    int gather;              // lane-chunks a stopped lane may idle before its warp runs the events
+                             // it gathered (0: no gathering), from the hop length (gather_chunks)
     double drift_abs;        // drift_tol * GM / Radii: the energy-drift guard's bound (0 = off)
     const float4 *face_f;    // FP32 icosphere tables (config model), or nullptr: FP64 descent
 };
@@ -94,6 +96,12 @@ struct FastCounters {
 size_t fast_slot_bytes(long long nslots, bool fp64 = false);
 size_t fast_inst_bytes();
 size_t fast_counter_bytes();
+// Expected steps of a typical hop: the ballistic flight time 2 v / g of a molecule launched at
+// the thermal speed sqrt(k_B T / m) of a 235 K surface, over the time step.
+double fast_hop_steps(const dsmc_params &p);
+// Event gathering of an instance from its typical hop (see fast_kernel): 16 lane-chunks below
+// 300 steps per hop, 4 below 600, none above.
+int gather_chunks(const dsmc_params &p);
 cudaError_t fast_fill_instance(const dsmc_params &p, const DevTables &t, long long pid_begin,
                                long long n, float *d_tab, size_t tab_floats, void *inst_host,
                                float *tab_host);
