@@ -594,10 +594,12 @@ __device__ __forceinline__ void horizon_add(const FastInst &I, int td, int fd, d
     atomicAdd(&I.t.horizon[td * I.p.ffd + fd], __double2ull_rn(W * DSMC_FIXED_SCALE));
 }
 
-// Old acceleration GM s / r^3 of a launch point (ballistic.c:176-181) and the hop's start.
+// Old acceleration GM s / r^3 of a launch point (ballistic.c:176-181) and the hop's start. The
+// energy baseline of the drift guard comes from e_launch when the launch already formed it.
 template <typename R>
 __device__ __forceinline__ void start_hop_state(const FastArgsT<R> &a, long long i,
-                                                const FastInst &I, HotT<R> &h) {
+                                                const FastInst &I, HotT<R> &h,
+                                                const double *e_launch) {
     if constexpr (is_f64<R>()) {
         const double sx = h.sh[0], sy = h.sh[1], sz = h.sh[2];
         const double ir = rsqrt(sx * sx + sy * sy + sz * sz);
@@ -614,7 +616,16 @@ __device__ __forceinline__ void start_hop_state(const FastArgsT<R> &a, long long
         h.oa[2] = g * sz;
     }
     h.hop = 0;
-    drift_start(a, i, I, h);
+    if (!e_launch) drift_start(a, i, I, h);
+    else if (I.drift_abs > 0.0) a.s.e0[i] = static_cast<float>(*e_launch);
+}
+
+// Orbital energy of a launch from the |v|^2 and |s|^2 its bound test formed: 1 / |s| as in
+// orbital_energy, so the baseline equals orbital_energy of the launched state.
+__device__ __forceinline__ double launch_energy(const FastInst &I, double v2, double r2) {
+    double ir = rsqrtf(static_cast<float>(r2));
+    ir = ir * (1.5 - 0.5 * r2 * ir * ir);
+    return 0.5 * v2 - I.p.GM * ir;
 }
 
 // Launch from the current surface position (ballistic.c:156-181; config: flux-weighted
@@ -635,6 +646,8 @@ __device__ bool launch(const FastArgsT<R> &a, long long i, const FastInst &I, Ho
     double s[3];
     get_pos(h, s);
     double vd[3];
+    double e_launch = 0.0;
+    bool have_e = false;
     if constexpr (is_f64<R>()) {
         if (!kCfg && p.model == DSMC_MODEL_REFERENCE) {
             // velocity_sample / velocity_sticking (velocity.c:49-73), ballistic.c:156-173
@@ -674,6 +687,8 @@ __device__ bool launch(const FastArgsT<R> &a, long long i, const FastInst &I, Ho
             const double v2 = vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2];
             const double rr = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
             if (v2 * v2 * rr < 4.0 * p.GM * p.GM) st.bound++;
+            e_launch = launch_energy(I, v2, rr);
+            have_e = true;
         }
     } else {
         float v[3];
@@ -725,13 +740,15 @@ __device__ bool launch(const FastArgsT<R> &a, long long i, const FastInst &I, Ho
                               static_cast<double>(v[2]) * v[2];
             const double rr = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
             if (v2 * v2 * rr < 4.0 * p.GM * p.GM) st.bound++;
+            e_launch = launch_energy(I, v2, rr);
+            have_e = true;
         }
         vd[0] = v[0];
         vd[1] = v[1];
         vd[2] = v[2];
     }
     set_vel(h, vd);
-    start_hop_state(a, i, I, h);
+    start_hop_state(a, i, I, h, have_e ? &e_launch : nullptr);
     return true;
 }
 
