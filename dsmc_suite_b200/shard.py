@@ -57,3 +57,15 @@ def allreduce_grids(dist, *grids: np.ndarray, device=None) -> list[np.ndarray]:
         res.append(out[k:k + g.size].reshape(g.shape).copy())
         k += g.size
     return res
+
+
+def sharded_solve(dist, solve_range, n: int, weak: bool = True, device=None) -> list[np.ndarray]:
+    """One rank's part of a sharded solve: the rank's particle-id range (weak scaling: n ids per
+    rank, `particle_range`; strong: n ids in all, `split_range`), solved by
+    solve_range(pid_begin, count) -> tuple of uint64 grids (density, horizon, optionally speed
+    histograms), then one all-reduce of all of them. Every rank returns the grids of one solve
+    of all ids. solve_range may run on the GPU (Context.run + density / horizon) or anywhere
+    else; `device` is the communication buffer's torch device ("cuda" for NCCL)."""
+    rank, world = dist.get_rank(), dist.get_world_size()
+    pid0, count = particle_range(rank, world, n) if weak else split_range(rank, world, n)
+    return allreduce_grids(dist, *solve_range(pid0, count), device=device)

@@ -86,9 +86,11 @@ def _rank_main(rank, world, port, model, out_dir):
             p = N.params_config(N.RUNNER_BALLISTIC)
             ico = N.Icosphere(3)
             S = N.SurfaceInputs(ico=ico, face_T=ico.face_temperature())
-        pid0, n = shard.particle_range(rank, world, N_PER_RANK)
-        r = O.run(p, S, n, pid_begin=pid0, nthreads=2, particles=False)
-        den, hor = shard.allreduce_grids(dist, r["density"], r["horizon"])
+        def solve_range(pid0, n):
+            r = O.run(p, S, n, pid_begin=pid0, nthreads=2, particles=False)
+            return r["density"], r["horizon"]
+
+        den, hor = shard.sharded_solve(dist, solve_range, N_PER_RANK)
         if rank == 0:
             np.savez(os.path.join(out_dir, "reduced.npz"), density=den, horizon=hor)
     finally:
@@ -260,6 +262,56 @@ def test_two_rank_reduction_keeps_uint64_words(tmp_path):
         assert got["a"].dtype == np.uint64 and got["a"].shape == (2, 2)
         np.testing.assert_array_equal(got["a"], want_a)
         np.testing.assert_array_equal(got["b"], want_b)
+
+
+def _rank_strong(rank, world, port, out_dir, n_total):
+    """Strong scaling: n_total ids split over the ranks (uneven), through sharded_solve."""
+    import sys
+    from datetime import timedelta
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    import torch.distributed as dist
+    from dsmc_suite_b200 import _native as N, shard
+    from oracle import oracle as O
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        p = N.params_config(N.RUNNER_BALLISTIC)
+        ico = N.Icosphere(3)
+        S = N.SurfaceInputs(ico=ico, face_T=ico.face_temperature())
+
+        def solve_range(pid0, n):
+            r = O.run(p, S, n, pid_begin=pid0, nthreads=2, particles=False)
+            return r["density"], r["horizon"]
+
+        den, hor = shard.sharded_solve(dist, solve_range, n_total, weak=False)
+        np.savez(os.path.join(out_dir, f"strong_{rank}.npz"), density=den, horizon=hor)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_strong_scaling_split_reduces_to_the_one_process_result(N, O, tmp_path):
+    """An odd number of ids split over two ranks (151 + 150): the reduced grids on every rank
+    equal one process solving all of them."""
+    import multiprocessing as mp
+    world, n_total = 2, 301
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_rank_strong, args=(r, world, port, str(tmp_path), n_total))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    p = N.params_config(N.RUNNER_BALLISTIC)
+    ico = N.Icosphere(3)
+    whole = O.run(p, N.SurfaceInputs(ico=ico, face_T=ico.face_temperature()), n_total, nthreads=2,
+                  particles=False)
+    for r in range(world):
+        got = np.load(tmp_path / f"strong_{r}.npz")
+        np.testing.assert_array_equal(got["density"], np.asarray(whole["density"]).reshape(got["density"].shape))
+        np.testing.assert_array_equal(got["horizon"], np.asarray(whole["horizon"]).reshape(got["horizon"].shape))
 
 
 def test_shard_ranges():
