@@ -48,7 +48,7 @@ constexpr size_t kCntOff = kVtOff + kVtBytes;
 constexpr size_t kCntBytes = round_up(23 * sizeof(int));
 constexpr size_t kFaceOff = kCntOff + kCntBytes;       // FP32 icosphere tables, up to 6 levels
 constexpr size_t kFaceBytes = round_up(4 * (20 + 3 * 27300 + 3 * 81920) * sizeof(float));
-constexpr size_t kScratchBytes = kFaceOff + kFaceBytes;   // about 9.9 MB
+constexpr size_t kScratchBytes = kFaceOff + kFaceBytes;   // about 10.0 MB
 
 // The scratch itself. In host code `g_scratch` names a host-side stand-in, not the device
 // memory: its device address comes from cudaGetSymbolAddress, once per device.

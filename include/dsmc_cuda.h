@@ -228,7 +228,7 @@ int dsmc_number_density_host(const dsmc_params *p, const uint64_t *density_fx, i
 /*            ADDS into them, so zero them first for a fresh result.                         */
 /*   stats    device [6] unsigned 64-bit counters in dsmc_stats order; zeroed by the call.   */
 /*   stream   a cudaStream_t, or NULL for the legacy default stream.                         */
-/* Scratch: one fixed device array of about 9.9 MB inside the library (at most 32,768       */
+/* Scratch: one fixed device array of about 10.0 MB inside the library (at most 32,768      */
 /* resident particle slots and (hd+1) + (ftd+1) + 2 (ffd+1) + 1 <= 4096 table floats, ftd  */
 /* and ffd <= 255). Every GPU that loads the library holds that array until the process     */
 /* exits. Larger grids are rejected with DSMC_ERR_INVALID. The first call on a device looks  */
