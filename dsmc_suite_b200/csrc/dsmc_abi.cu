@@ -246,6 +246,9 @@ int dsmc_run(dsmc_ctx *c, int path, int64_t pid_begin, int64_t n) {
                 c->fast = new (std::nothrow) dsmc::FastEngine();
                 if (!c->fast) return fail(c, DSMC_ERR_NO_MEMORY, "host allocation failed");
             }
+            if (path == DSMC_PATH_FAST_FP64 && c->fast->block != 128)
+                return fail(c, DSMC_ERR_INVALID, "FAST_FP64 runs 128-thread blocks (launch shape has %d)",
+                            c->fast->block);
             cudaError_t e = c->fast->run(c->params, c->t, path == DSMC_PATH_FAST_FP64, pid_begin, n,
                                          c->num_sms, c->stream);
             c->last_launches = c->fast->launches;

@@ -327,3 +327,13 @@ def test_abi_error_paths(N, built):
             c.setup(bad, N.SurfaceInputs(T_map=np.zeros((36, 72))))
         with pytest.raises(DsmcError):
             N.check(N.lib().dsmc_set_launch_shape(c.h, 100, 0, 10, 1), "shape", c.h)
+        # FAST_FP64 runs 128-thread blocks only: a 256-thread shape is refused with a message
+        p = N.params_config(N.RUNNER_BALLISTIC)
+        ico = N.Icosphere(3)
+        c.setup(p, N.SurfaceInputs(ico=ico, face_T=ico.face_temperature()))
+        N.check(N.lib().dsmc_set_launch_shape(c.h, 256, 0, 2048, 1), "shape", c.h)
+        with pytest.raises(DsmcError) as e:
+            c.run(N.PATH_FAST_FP64, 0, 100)
+        assert e.value.status == -1 and "128-thread" in str(e.value)
+        c.run(N.PATH_FAST_FP32, 0, 100)      # the FP32 engine takes the shape
+        c.sync()
