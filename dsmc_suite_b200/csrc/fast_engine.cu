@@ -361,67 +361,74 @@ __device__ __forceinline__ void move_cell(const FastInst &I, HotT<R> &h, BoundsT
                                           R r2, R zz, bool in_r, bool in_t, bool in_f) {
     int ht = h.cell >> 16, td = (h.cell >> 8) & 0xff, fd = h.cell & 0xff;
     // the three walks are independent (shells by r^2, rows by z|z| / r^2, columns by the
-    // longitude tests), so a coordinate still inside its two bounds needs no walk
+    // longitude tests), so a coordinate still inside its two bounds needs no walk. Each walk
+    // goes one way only: after a move up the old upper bound is the new lower one, which the
+    // particle is above, so the downward test cannot pass (and the other way round); the
+    // walks test one bound per move (same cells as testing both).
     if (!in_r) {
         const int hd = I.p.hd;
         const R *rb2 = Tables<R>::rb2(I);
-        for (int it = 0; it < 64; it++) {
-            if (r2 > b.r2hi && ht + 1 < hd) {
+        if (r2 > b.r2hi) {
+            for (int it = 0; it < 64 && r2 > b.r2hi && ht + 1 < hd; it++) {
                 ht++;
                 b.r2lo = b.r2hi;
                 b.r2hi = __ldg(rb2 + ht + 1);
-            } else if (r2 <= b.r2lo && ht > 0) {
+            }
+        } else {
+            for (int it = 0; it < 64 && r2 <= b.r2lo && ht > 0; it++) {
                 ht--;
                 b.r2hi = b.r2lo;
                 b.r2lo = __ldg(rb2 + ht);
-            } else {
-                break;
             }
         }
     }
     if (!in_t) {
         const int ftd = I.p.ftd;
         const R *sbs = Tables<R>::sbs(I);
-        for (int it = 0; it < 64; it++) {
-            if (zz > r2 * b.zhi && td + 1 < ftd) {
+        if (zz > r2 * b.zhi) {
+            for (int it = 0; it < 64 && zz > r2 * b.zhi && td + 1 < ftd; it++) {
                 td++;
                 b.zlo = b.zhi;
                 b.zhi = __ldg(sbs + td + 1);
-            } else if (zz <= r2 * b.zlo && td > 0) {
+            }
+        } else {
+            for (int it = 0; it < 64 && zz <= r2 * b.zlo && td > 0; it++) {
                 td--;
                 b.zhi = b.zlo;
                 b.zlo = __ldg(sbs + td);
-            } else {
-                break;
             }
         }
     }
     if (!in_f) {
         const int ffd = I.p.ffd;
         const typename Tables<R>::V2 *lonb = Tables<R>::lonb(I);
-        for (int it = 0; it < 512; it++) {
-            if (x * b.c1 - y * b.s1 > R(0)) {
+        if (x * b.c1 - y * b.s1 > R(0)) {
+            for (int it = 0; it < 512 && x * b.c1 - y * b.s1 > R(0); it++) {
                 fd = fd + 1 == ffd ? 0 : fd + 1;
                 b.s0 = b.s1;
                 b.c0 = b.c1;
                 const auto q = __ldg(lonb + fd + 1);
                 b.s1 = q.x;
                 b.c1 = q.y;
-            } else if (x * b.c0 - y * b.s0 <= R(0) && !(fd == 0 && x >= R(0) && y > R(0))) {
+            }
+        } else {
+            for (int it = 0; it < 512 && x * b.c0 - y * b.s0 <= R(0) && !(fd == 0 && x >= R(0) && y > R(0));
+                 it++) {
                 fd = fd == 0 ? ffd - 1 : fd - 1;
                 b.s1 = b.s0;
                 b.c1 = b.c0;
                 const auto q = __ldg(lonb + fd);
                 b.s0 = q.x;
                 b.c0 = q.y;
-            } else {
-                break;
             }
         }
     }
     const int cell = pack_cell(ht, td, fd);
     if (cell == h.cell) return;
-    flush_cell(I, h);
+    // the run of a flying particle has a cell and no negative weight: flushed without the tests
+    // of flush_cell (a run of zero adds zero)
+    atomicAdd(&I.t.density[h.ci], fixed_of(h.run_w));
+    h.run_w = R(0);
     h.cell = cell;
     h.ci = (ht * I.p.ftd + td) * I.p.ffd + fd;
     h.W = h.w0 * exp2_r<R>(-c_day_of<R>(I) * static_cast<R>(h.nday));   // re-anchor the running weight
