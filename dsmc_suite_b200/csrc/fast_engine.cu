@@ -1905,22 +1905,6 @@ cudaError_t FastEngine::run(const dsmc_params &p, const DevTables &t, bool fp64,
     return drain(n, stream);
 }
 
-cudaError_t FastEngine::run_batch(const std::vector<dsmc_params> &ps, const std::vector<DevTables> &ts,
-                                  const std::vector<long long> &counts, int num_sms, cudaStream_t stream) {
-    for (const auto &p : ps)
-        if (p.ftd > 255 || p.ffd > 255 || p.hd > 32767) return cudaErrorInvalidValue;
-    fp64_ = false;
-    mode_ = launch_mode(ps, ts);
-    cudaError_t e = ensure_slots(num_sms);
-    if (e != cudaSuccess) return e;
-    std::vector<long long> pid0(ps.size(), 0);
-    e = upload_instances(ps, ts, counts, pid0, stream);
-    if (e != cudaSuccess) return e;
-    long long total = 0;
-    for (long long c : counts) total += c;
-    return drain(total, stream);
-}
-
 cudaError_t FastEngine::serve_open(int num_sms, int max_instances, cudaStream_t stream) {
     if (max_instances < 1) return cudaErrorInvalidValue;
     fp64_ = false;   // serving runs the FP32 engine

@@ -123,10 +123,6 @@ public:
     cudaError_t run(const dsmc_params &p, const DevTables &t, bool fp64, long long pid_begin,
                     long long n, int num_sms, cudaStream_t stream);
 
-    // Batched solve: many instances in one queue (tables and outputs per instance).
-    cudaError_t run_batch(const std::vector<dsmc_params> &ps, const std::vector<DevTables> &ts,
-                          const std::vector<long long> &counts, int num_sms, cudaStream_t stream);
-
     void set_shape(int blk, int per_sm, int k, int g) {
         if (blk != block || per_sm != blocks_per_sm) nslots_want_changed_ = true;
         block = blk;
@@ -194,7 +190,7 @@ private:
     Slots slots_{};
     SlotsT<double> slots64_{};                // the same memory carved for FP64 state
     void *slot_mem_ = nullptr;
-    bool fp64_ = false;                       // precision of run / run_batch launches
+    bool fp64_ = false;                       // precision of run launches
     bool slot_fp64_ = false;                  // precision the slot memory is carved for
     long long nslots_ = 0;
     FastInst *d_inst_ = nullptr;
@@ -210,7 +206,7 @@ private:
     int graph_key_[4] = {0, 0, 0, 0};
     bool nslots_want_changed_ = false;
     int variant_ = 2;
-    int mode_ = 0;   // loop of run / run_batch launches (see fast_kernel)
+    int mode_ = 0;   // loop of run launches (see fast_kernel)
 };
 
 }  // namespace dsmc
