@@ -198,11 +198,16 @@ int publish_pending(dsmc_server *s) {
         order.emplace_back(-dsmc::fast_hop_steps(s->reqs[static_cast<size_t>(tk)]->prob->p), tk);
     std::stable_sort(order.begin(), order.end(),
                      [](const auto &a, const auto &b) { return a.first < b.first; });
-    for (const auto &o : order) {
-        Request &q = *s->reqs[static_cast<size_t>(o.second)];
+    for (size_t k = 0; k < order.size(); k++) {
+        Request &q = *s->reqs[static_cast<size_t>(order[k].second)];
         const cudaError_t e = s->engine.serve_append(q.prob->p, q.prob->t, q.n, &q.inst, s->upload, s->compute);
-        if (e != cudaSuccess) return cuda_fail(s, "appending to the work queue", e);
-        s->active.push_back(o.second);
+        if (e != cudaSuccess) {
+            // the requests not yet in the queue stay pending, in their queue order
+            s->pending.clear();
+            for (size_t j = k; j < order.size(); j++) s->pending.push_back(order[j].second);
+            return cuda_fail(s, "appending to the work queue", e);
+        }
+        s->active.push_back(order[k].second);
         if (q.mode == 0) s->general_active++;
         if (q.mode == 2) s->collide_active++;
     }
