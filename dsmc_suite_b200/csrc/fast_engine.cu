@@ -601,8 +601,9 @@ __device__ __forceinline__ void horizon_add(const FastInst &I, int td, int fd, d
     atomicAdd(&I.t.horizon[td * I.p.ffd + fd], __double2ull_rn(W * DSMC_FIXED_SCALE));
 }
 
-// Old acceleration GM s / r^3 of a launch point (ballistic.c:176-181) and the hop's start. The
-// energy baseline of the drift guard comes from e_launch when the launch already formed it.
+// Old acceleration GM s / r^3 of a launch point (ballistic.c:176-181; the FP32 engine keeps it
+// times dt) and the hop's start. The energy baseline of the drift guard comes from e_launch when
+// the launch already formed it.
 template <typename R>
 __device__ __forceinline__ void start_hop_state(const FastArgsT<R> &a, long long i,
                                                 const FastInst &I, HotT<R> &h,
@@ -617,7 +618,7 @@ __device__ __forceinline__ void start_hop_state(const FastArgsT<R> &a, long long
     } else {
         const float sx = h.sh[0] + h.sl[0], sy = h.sh[1] + h.sl[1], sz = h.sh[2] + h.sl[2];
         const float ir = rsqrtf(fmaf(sx, sx, fmaf(sy, sy, sz * sz)));
-        const float g = static_cast<float>(I.p.GM) * (ir * ir * ir);
+        const float g = static_cast<float>(I.p.GM * I.p.dt_step) * (ir * ir * ir);
         h.oa[0] = g * sx;
         h.oa[1] = g * sy;
         h.oa[2] = g * sz;
@@ -1174,9 +1175,11 @@ __device__ bool start_next(const FastArgsT<R> &a, long long i, HotT<R> &h, Bound
     }
 }
 
-// One Verlet step of the reference's variant. FP32: (hi, lo) position and velocity sums; FP64:
-// plain doubles. (x, y, z, r2) hold the current position on entry and the new one on exit; d the
-// displacement.
+// One Verlet step of the reference's variant. FP32: (hi, lo) position and velocity sums, and the
+// acceleration carried as the velocity change a * dt (GM passed as GM dt, c1 = 1.5 dt,
+// c2 = dt / 6; three multiplies fewer per step, and at a power-of-two dt the same roundings as
+// a and dt kept apart); FP64: plain doubles with c1 = 1.5 dt^2, c2 = dt^2 / 6. (x, y, z, r2)
+// hold the current position on entry and the new one on exit; d the displacement.
 __device__ __forceinline__ void verlet_step(Hot &h, float &x, float &y, float &z, float &r2,
                                             float GM, float dt, float c1, float c2, float d[3]) {
     const float ir = rsqrtf(r2);
@@ -1186,7 +1189,7 @@ __device__ __forceinline__ void verlet_step(Hot &h, float &x, float &y, float &z
     for (int k = 0; k < 3; k++) {
         d[k] = fmaf(h.vh[k], dt, fmaf(h.vl[k], dt, -fmaf(acc[k], c1, h.oa[k] * c2)));
         accumulate(h.sh[k], h.sl[k], d[k]);
-        accumulate(h.vh[k], h.vl[k], -acc[k] * dt);
+        accumulate(h.vh[k], h.vl[k], -acc[k]);
         h.oa[k] = acc[k];
     }
     x = h.sh[0] + h.sl[0];
@@ -1264,14 +1267,17 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) fast_kernel(const Fas
             cur = h.inst;
             I = &a.inst[cur];
             const dsmc_params &p = I->p;
-            GM = static_cast<R>(p.GM);
             dt = static_cast<R>(p.dt_step);
-            c1 = static_cast<R>(1.5 * p.dt_step * p.dt_step);
-            c2 = static_cast<R>(p.dt_step * p.dt_step / 6.0);
             if constexpr (is_f64<R>()) {
+                GM = p.GM;
+                c1 = 1.5 * p.dt_step * p.dt_step;
+                c2 = p.dt_step * p.dt_step / 6.0;
                 rl2 = p.Radii * p.Radii;
                 re2 = p.max_height * p.max_height;
             } else {
+                GM = static_cast<R>(p.GM * p.dt_step);
+                c1 = static_cast<R>(1.5 * p.dt_step);
+                c2 = static_cast<R>(p.dt_step / 6.0);
                 rl2 = I->r_land2;
                 re2 = I->r_esc2;
             }
@@ -1425,10 +1431,10 @@ __global__ void push_fp32_kernel(const dsmc_params p, long long n, int nsteps, d
     set_vel(h, v);
     const double R0 = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
     const double g0 = p.GM / (R0 * R0 * R0);
-    for (int k = 0; k < 3; k++) h.oa[k] = static_cast<float>(g0 * s[k]);
-    const float GM = static_cast<float>(p.GM), dt = static_cast<float>(p.dt_step);
-    const float c1 = static_cast<float>(1.5 * p.dt_step * p.dt_step);
-    const float c2 = static_cast<float>(p.dt_step * p.dt_step / 6.0);
+    for (int k = 0; k < 3; k++) h.oa[k] = static_cast<float>(g0 * s[k] * p.dt_step);
+    const float GM = static_cast<float>(p.GM * p.dt_step), dt = static_cast<float>(p.dt_step);
+    const float c1 = static_cast<float>(1.5 * p.dt_step);
+    const float c2 = static_cast<float>(p.dt_step / 6.0);
     const float rl2 = static_cast<float>(p.Radii * p.Radii);
     const float re2 = static_cast<float>(p.max_height * p.max_height);
     float x = h.sh[0] + h.sl[0], y = h.sh[1] + h.sl[1], z = h.sh[2] + h.sl[2];

@@ -49,6 +49,7 @@ struct SlotsT {
     unsigned *pid;           // particle id within its instance
     unsigned *evt;           // Philox event counter
     R *sh, *sl, *vh, *vl, *oa;   // [3][S] each: position hi/lo, velocity hi/lo, old accel
+                                 // (times dt in the FP32 engine)
     R *w0;                   // weight factor outside photolysis
     int *nday;               // day-side steps (photolysis exponent)
     int *steps;              // steps in the particle's life
