@@ -36,7 +36,13 @@ CUDA_SOURCES = {
     "kernel_fit.cu": ["-fmad=false"],
     "kernel_thermal.cu": ["-fmad=false"],
     "kernel_raytrace.cu": ["-fmad=false"],
-    "fast_engine.cu": [],
+    # FP32 subnormals flushed to zero: the FAST engines' FP32 values (positions, velocities and
+    # their two-sum low words, weights above the photolysis cutoff, cell-test products) are far
+    # from the subnormal range, and the per-step reciprocal square root then needs no subnormal
+    # guard. Grids of the config workloads are bit-identical to the build without the flag; the
+    # reference model's FP32 event maps (asinf, atan2f, sincosf) change at the last place. The
+    # Ceres-like workload runs 2.23e11 particle-steps/s against 2.09e11 without it.
+    "fast_engine.cu": ["-ftz=true"],
     "kernel_peak.cu": [],
     "noalloc.cu": [],
     "problem.cu": [],
@@ -83,7 +89,9 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
     (PKG / "bin").mkdir(exist_ok=True)
     nvcc, gcc = _tool("nvcc"), _tool("gcc")
-    headers = list(INC.glob("*.h")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh"))
+    # objects depend on the headers and on this file (its flags), so a flag change rebuilds
+    headers = (list(INC.glob("*.h")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) +
+               [Path(__file__).resolve()])
     objs = []
     for src, extra in CUDA_SOURCES.items():
         s = CSRC / src
